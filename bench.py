@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""Headline benchmark: S-matrices/s of the RGF slice recursion, 2D N=1024,
+L=4096 (the config-2 structure of rgf_b200.workloads), complex FP64 plain form.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one full S-matrix (204 x 204) of the config-2 structure.
+
+* value  : S-matrices/s with epsilon and S resident in HBM, device-timed
+           (CUDA events on the stream the library launches on), L2 flushed
+           (256 MiB write) between steps, max over ranks.
+* e2e    : the same through the C ABI with pinned HOST epsilon and S; the
+           timed region includes the 64 MiB H2D of epsilon and the D2H of S.
+* roofline: the dominant kernel (the sweep's rank-32 FP64 DMMA update),
+           sampled with CUDA events every 64th slice; peak = FP64 DMMA rate
+           measured on this pool's B200s (profiles/fp64_dmma_peak.md).
+* cpu_baseline: the numpy/scipy oracle (restatement of the MATLAB reference;
+           MATLAB itself is not installed) on the host cores, on a bounded
+           sample of slices, extrapolated linearly in L.
+* --impl reference: that CPU oracle timed alone, same metric and config.
+
+Multi-GPU (torchrun): replicas only -- each rank computes its own S-matrices;
+the path has no collective.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "S-matrices/s 2D N=1024 L=4096: 3xTF32+refine vs FP64 at 1e-10 rel err; grad/fwd"
+UNIT = "S-matrices/s"
+FP64_DMMA_PEAK_TFLOPS = 37.0  # measured on this pool, profiles/fp64_dmma_peak.md
+PROFILE_EVERY = 64
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only)
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(minutes=20),
+                                    device_id=torch.device("cuda", self.local_rank))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[5:9]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i, v in enumerate(r[3]) if v.lower() == "active"})
+        load = [r[0] for r in rows if r[2] > 300.0] or [r[0] for r in rows]
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": max(r[1] for r in rows),
+                "power_w_max": max(r[2] for r in rows), "samples": len(rows), "reasons": reasons}
+
+
+# ---------------------------------------------------------------------------
+# CPU oracle timing (test infrastructure; only the baseline legs touch it)
+# ---------------------------------------------------------------------------
+def cpu_oracle_rate(syst, out, in_, n_slices_sample: int):
+    """Time the oracle on the first n slices and on zero slices; extrapolate
+    linearly to the full L.  Returns (S-matrices/s, seconds per slice, setup s)."""
+    from oracle.rgf_ref import cal_smatrix_RGF
+    eps = syst["epsilon"]
+    L = eps.shape[1]
+    s0 = dict(syst, epsilon=eps[:, :0])
+    t = time.perf_counter()
+    cal_smatrix_RGF(s0, out, in_)
+    t_setup = time.perf_counter() - t
+    s1 = dict(syst, epsilon=eps[:, :n_slices_sample])
+    t = time.perf_counter()
+    cal_smatrix_RGF(s1, out, in_)
+    t_n = time.perf_counter() - t
+    per_slice = max(t_n - t_setup, 1e-9) / n_slices_sample
+    return 1.0 / (t_setup + per_slice * L), per_slice, t_setup
+
+
+def run_reference(args, dist):
+    if dist.rank != 0:
+        return
+    from rgf_b200 import workloads
+    syst, out, in_ = workloads.config2()
+    cores = os.cpu_count()
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, per_slice, setup = cpu_oracle_rate(syst, out, in_, args.ref_slices)
+        if i >= args.warmup:
+            vals.append(v)
+    value = statistics.mean(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic: seeded config-2 structure (rgf_b200.workloads.config2)",
+            "config": config_dict(),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"numpy/scipy FP64 restatement of cal_smatrix_RGF.m (MATLAB not installed): "
+                                       f"{args.ref_slices} of 4096 slices + lead set-up per step, "
+                                       f"extrapolated linearly in L; OpenBLAS threads={cores}"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def config_dict():
+    return {"workload": "config2: 2D Dirichlet, N=1024 transverse sites, L=4096 slices, eps 2.25 + 30% disks "
+                        "(r 4-12 px) of 1 + 1j*U[0,0.01), k0dx=2pi/20, full S (P=102 per side, 204x204)",
+            "form": "fp64 plain (complex FP64 throughout, FP64 DMMA tensor cores)",
+            "N": 1024, "L": 4096, "P_per_side": 102, "l2": "flushed between steps (256 MiB write)",
+            "parallelism": "replicas (independent S-matrices per GPU, no collective)"}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, dist):
+    import torch
+
+    from rgf_b200 import _abi, workloads
+    dev = dist.local_rank
+    torch.cuda.set_device(dev)
+    syst, out, in_ = workloads.config2()
+    if args.slices:
+        syst = dict(syst, epsilon=np.ascontiguousarray(syst["epsilon"][:, :args.slices]))
+    ny, nx = syst["epsilon"].shape
+    eps_host = torch.from_numpy(np.ascontiguousarray(syst["epsilon"].ravel(order="F"))).pin_memory()
+    eps_dev = eps_host.to(f"cuda:{dev}")
+    h = _abi.Handle(dev)
+    stream = torch.cuda.current_stream()
+    h.set_stream(stream.cuda_stream)
+    lib = h.lib
+    req = _abi.Request(None, _abi.RGF_ALL, None, _abi.RGF_ALL, None, _abi.RGF_ALL, None, _abi.RGF_ALL)
+
+    def syst_struct(eps_ptr, on_dev):
+        return _abi.Syst2D(ny, nx, eps_ptr, on_dev, _abi.cplx(1.0), _abi.cplx(1.0), _abi.cplx(syst["k0dx"]),
+                           _abi.BC_DIRICHLET, 0.0)
+
+    no, ni = ctypes.c_int64(), ctypes.c_int64()
+    sd = syst_struct(eps_dev.data_ptr(), 1)
+    _abi.check(lib.rgf_smatrix_size_2d(h.h, ctypes.byref(sd), ctypes.byref(req), ctypes.byref(no), ctypes.byref(ni)))
+    n_out, n_in = no.value, ni.value
+    S_dev = torch.zeros((n_in, n_out), dtype=torch.complex128, device=f"cuda:{dev}")  # column-major n_out x n_in
+    S_host = torch.zeros((n_in, n_out), dtype=torch.complex128).pin_memory()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{dev}")
+
+    def step(device_io: bool, profile: int):
+        opt = _abi.Options(_abi.RGF_FP64, 0, 1 if device_io else 0, profile)
+        s = syst_struct(eps_dev.data_ptr() if device_io else eps_host.data_ptr(), 1 if device_io else 0)
+        Sp = S_dev.data_ptr() if device_io else S_host.data_ptr()
+        _abi.check(lib.rgf_smatrix_2d(h.h, ctypes.byref(s), ctypes.byref(req), ctypes.byref(opt), Sp, n_out, None))
+
+    def timed(device_io: bool, k: int, profile: int):
+        total_ms, prof = 0.0, [0, 0.0, 0.0, ""]
+        for _ in range(k):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step(device_io, profile)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            total_ms += e0.elapsed_time(e1)
+            if profile:
+                n, ms, fl, name = h.profile()
+                prof[0] += n
+                prof[1] += ms
+                prof[2] = fl
+                prof[3] = name
+        return total_ms, prof
+
+    for _ in range(args.warmup):
+        step(True, 0)
+    torch.cuda.synchronize()
+    dist.barrier()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    torch.cuda.synchronize()
+    dist.barrier()
+    t_ms, prof = timed(True, args.steps, PROFILE_EVERY)
+    launches, _ = h.stats()
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    t_ms = dist.max(t_ms)
+    # end-to-end through the C ABI with host buffers
+    dist.barrier()
+    e_ms, _ = timed(False, args.steps, 0)
+    dist.barrier()
+    e_ms = dist.max(e_ms)
+    value = args.steps * dist.world / (t_ms / 1e3)
+    e2e = args.steps * dist.world / (e_ms / 1e3)
+
+    S = S_dev.cpu().numpy().T  # n_out x n_in
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic: seeded config-2 structure (rgf_b200.workloads.config2); no dataset exists",
+            "config": config_dict()}
+    F = workloads.canonical_flops(1024, 4096, 102, 102)
+    line["slices_per_s"] = value * 4096
+    line["canonical_flops_per_S"] = F
+    line["canonical_tflops"] = F * value / 1e12 / dist.world
+    line["precision_form"] = None
+    line["grad_over_fwd"] = None
+    n, ms, fl, name = prof
+    achieved = fl / (ms / n / 1e3) / 1e12 if n else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get("sweep_update_bytes_per_launch")
+    line["roofline"] = {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": FP64_DMMA_PEAK_TFLOPS,
+                        "unit": "TFLOP/s", "frac": (achieved / FP64_DMMA_PEAK_TFLOPS) if achieved else None,
+                        "traffic": traffic, "flops_per_launch": fl, "timed_launches": n,
+                        "peak_source": "FP64 DMMA (mma.sync f64) microbenchmark on this pool's B200, burst "
+                                       "(MEASURED_PEAKS.json has no FP64 figure)"}
+    line["e2e"] = {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(eps_host.numel() * 16),
+                   "d2h_bytes_per_step": int(n_out * n_in * 16)}
+    line["gpu_launches"] = int(launches) * args.steps
+    line["clocks"] = clk
+    # accuracy of this run's S against the committed oracle fixture (if present)
+    gpath = os.path.join(ROOT, "tests", "golden", "cfg2.npz")
+    if args.slices:
+        line["config"]["workload"] = f"PROFILING ONLY: config2 truncated to {args.slices} slices"
+    elif os.path.exists(gpath):
+        S0 = np.load(gpath, allow_pickle=True)["S"]
+        line["rel_err_vs_oracle"] = float(np.linalg.norm(S - S0) / np.linalg.norm(S0))
+    line["reciprocity_err"] = float(np.abs(S - S.T).max())
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        cores = os.cpu_count()
+        v, per_slice, setup = cpu_oracle_rate(syst, out, in_, args.ref_slices)
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": f"numpy/scipy FP64 restatement of cal_smatrix_RGF.m (MATLAB not "
+                                          f"installed): lead set-up + {args.ref_slices} of 4096 slices, "
+                                          f"extrapolated linearly in L ({per_slice * 1e3:.1f} ms/slice); "
+                                          f"OpenBLAS threads={cores}"}
+    h.close()
+    if dist.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-slices", type=int, default=32)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--slices", type=int, default=0,
+                    help="profiling only: keep the first n slices (the JSON line is then not a bench number)")
+    args = ap.parse_args()
+    dist = Dist() if args.impl == "ours" else None
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank == 0:
+            class _D:
+                rank = 0
+            run_reference(args, _D())
+        return
+    try:
+        run_ours(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,190 @@
+/*
+ * rgf.h -- C ABI of librgf, a B200 (sm_100a) implementation of the recursive
+ * Green's function (RGF) slice recursion of chiaweihsu/RGF.
+ *
+ * Every entry point replaces one MATLAB function of the reference:
+ *
+ *   rgf_smatrix_2d          <- src/cal_smatrix_RGF.m:1      [smatrix, channels] = cal_smatrix_RGF(syst, out, in)
+ *   rgf_smatrix_3d          <- src/cal_smatrix_RGF_3D.m:1   [smatrix, channels] = cal_smatrix_RGF_3D(syst, out, in)
+ *   rgf_setup_channels_2d   <- src/setup_channels.m:1       channels = setup_channels(ny, BC, k0dx, epsilon_L, epsilon_R)
+ *   rgf_setup_channels_3d   <- src/setup_channels_3D.m:1    channels = setup_channels_3D(nx, ny, BC, k0dx, epsilon_L, epsilon_R)
+ *   rgf_build_laplacian_1d  <- src/build_laplacian_1d.m:1   A = build_laplacian_1d(n, BC)
+ *
+ * The reference has no FFI of its own (it is MATLAB source); the binding a
+ * MATLAB user calls is a MEX gateway over this header (matlab/rgf_mex.c).
+ *
+ * Conventions
+ *  - Complex numbers are rgf_cplx {re, im}: the memory layout of C99
+ *    double _Complex, numpy complex128 and MATLAB's interleaved complex API.
+ *  - Arrays are column-major (MATLAB layout).  syst.epsilon of size [ny, nx]
+ *    (2D) or [nx, ny, nz] (3D) is passed as the plain column-major buffer,
+ *    so slice n is the contiguous block epsilon + n*N, N = ny (2D) or nx*ny (3D).
+ *  - Channel indices in the C ABI are 0-based (MATLAB's are 1-based; the
+ *    MEX gateway and the Python wrapper convert).
+ *  - All buffers are owned by the caller.  A handle owns its device
+ *    workspace and CUDA stream; one handle per host thread.  Calls on
+ *    distinct handles are independent.
+ *  - Every function returns an rgf_status; rgf_last_error() gives the
+ *    message of the last failure on the calling thread.
+ */
+#ifndef RGF_H
+#define RGF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RGF_API __attribute__((visibility("default")))
+#else
+#define RGF_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  double re, im;
+} rgf_cplx;
+
+typedef enum {
+  RGF_OK = 0,
+  RGF_ERR_ARG = 1,       /* invalid argument (MATLAB error() in the reference)          */
+  RGF_ERR_NONFINITE = 2, /* NaN/Inf in epsilon, epsilon_L/R or k0dx                      */
+  RGF_ERR_SINGULAR = 3,  /* a pivot block of a slice matrix is singular/ill-conditioned */
+  RGF_ERR_TIMEOUT = 4,   /* a device-side wait gave up (bounded spin)                    */
+  RGF_ERR_CUDA = 5,      /* CUDA runtime error                                           */
+  RGF_ERR_OOM = 6,       /* device allocation failed                                     */
+  RGF_ERR_NODEVICE = 7   /* no usable CUDA device                                        */
+} rgf_status;
+
+/* Transverse boundary conditions (setup_channels.m:10-20, build_laplacian_1d.m:9-17). */
+typedef enum {
+  RGF_BC_PERIODIC = 0,          /* 'periodic'                      */
+  RGF_BC_DIRICHLET = 1,         /* 'Dirichlet' / 'PEC'             */
+  RGF_BC_NEUMANN = 2,           /* 'Neumann' / 'PMC'               */
+  RGF_BC_DIRICHLET_NEUMANN = 3, /* 'DirichletNeumann' / 'PECPMC'   */
+  RGF_BC_NEUMANN_DIRICHLET = 4, /* 'NeumannDirichlet' / 'PMCPEC'   */
+  RGF_BC_BLOCH = 5              /* numeric BC = k*a (Bloch phase)  */
+} rgf_bc;
+
+/* Numeric form of the slice recursion. */
+typedef enum {
+  RGF_FP64 = 0 /* complex FP64 throughout (the drop-in form) */
+} rgf_precision;
+
+/* Value of n_* in rgf_request meaning "all propagating channels on that side"
+ * (the MATLAB cell form {'left'} / {'right'}, cal_smatrix_RGF.m:120-135). */
+#define RGF_ALL (-1)
+
+typedef struct rgf_handle_s* rgf_handle;
+
+/* syst for cal_smatrix_RGF (cal_smatrix_RGF.m:12-34). */
+typedef struct {
+  int64_t ny, nx;            /* size(syst.epsilon) = [ny, nx]; ny >= 1, nx >= 0          */
+  const rgf_cplx* epsilon;   /* ny*nx, column-major; host memory unless eps_on_device    */
+  int32_t eps_on_device;     /* 1: epsilon is a device pointer on the handle's device    */
+  rgf_cplx epsilon_L, epsilon_R, k0dx;
+  int32_t yBC;               /* rgf_bc                                                   */
+  double ka;                 /* Bloch phase ky*a (yBC == RGF_BC_BLOCH)                   */
+} rgf_syst2d;
+
+/* syst for cal_smatrix_RGF_3D (cal_smatrix_RGF_3D.m:12-31). */
+typedef struct {
+  int64_t nx, ny, nz;        /* size(syst.epsilon) = [nx, ny, nz]                        */
+  const rgf_cplx* epsilon;   /* nx*ny*nz, column-major (x fastest)                       */
+  int32_t eps_on_device;
+  rgf_cplx epsilon_L, epsilon_R, k0dx;
+  int32_t xyBC;              /* RGF_BC_PERIODIC, RGF_BC_DIRICHLET or RGF_BC_BLOCH        */
+  double kxa, kya;           /* Bloch phases (xyBC == RGF_BC_BLOCH)                      */
+} rgf_syst3d;
+
+/* out / in of cal_smatrix_RGF (cal_smatrix_RGF.m:35-50, 103-178): 0-based
+ * channel lists per side; n == RGF_ALL selects every propagating channel,
+ * n == 0 selects none. */
+typedef struct {
+  const int64_t* ind_out_L; int64_t n_out_L;
+  const int64_t* ind_out_R; int64_t n_out_R;
+  const int64_t* ind_in_L;  int64_t n_in_L;
+  const int64_t* ind_in_R;  int64_t n_in_R;
+} rgf_request;
+
+typedef struct {
+  int32_t precision;  /* rgf_precision (0 = RGF_FP64)                                  */
+  int32_t block;      /* reserved: pivot-block width of the slice inverse (0 = default)*/
+  int32_t S_on_device;/* 1: S is a device pointer (no D2H copy)                        */
+  int32_t profile;    /* > 0: time the dominant kernel with CUDA events on every
+                         profile-th slice (read back with rgf_last_profile)           */
+} rgf_options;
+
+/* channels struct (setup_channels.m:30-82).  All pointers are caller-owned
+ * arrays of capacity N (N = ny in 2D, nx*ny in 3D); any may be NULL. */
+typedef struct {
+  double* kydx;            /* N: transverse ky*dx (3D: nx-by-ny column-major)           */
+  double* kxdx_t;          /* 3D only: transverse kx*dx (nx-by-ny column-major)         */
+  rgf_cplx* kxdx_L;        /* N: longitudinal wavenumber, left (2D kxdx / 3D kzdx)      */
+  rgf_cplx* kxdx_R;        /* N: right                                                  */
+  rgf_cplx* sqrt_mu_L;     /* first N_prop_L entries used                               */
+  rgf_cplx* sqrt_mu_R;
+  int64_t* ind_prop_L;     /* 0-based, first N_prop_L entries used                      */
+  int64_t* ind_prop_R;
+  int64_t* ind_prop_conj_L;/* 0-based permutation of 0..N_prop_L-1 (2D, real profiles or ka == 0) */
+  int64_t* ind_prop_conj_R;
+  int64_t N_prop_L, N_prop_R;  /* outputs; N_prop_R = -1 for a one-sided setup          */
+  int32_t has_prop_conj;       /* output: 1 if ind_prop_conj_* were written             */
+  int32_t reserved;
+} rgf_channels;
+
+/* ---- handle ---------------------------------------------------------------- */
+RGF_API rgf_status rgf_create(int device, rgf_handle* out);
+RGF_API rgf_status rgf_destroy(rgf_handle h);
+
+/* ---- cal_smatrix_RGF / cal_smatrix_RGF_3D ----------------------------------- */
+/* S: n_out x n_in, column-major with leading dimension ldS >= n_out, where
+ * rows are [out_L ; out_R] and columns [in_L ; in_R] (cal_smatrix_RGF.m:56-61).
+ * ch may be NULL. */
+RGF_API rgf_status rgf_smatrix_2d(rgf_handle h, const rgf_syst2d* syst, const rgf_request* req,
+                          const rgf_options* opt, rgf_cplx* S, int64_t ldS, rgf_channels* ch);
+RGF_API rgf_status rgf_smatrix_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_request* req,
+                          const rgf_options* opt, rgf_cplx* S, int64_t ldS, rgf_channels* ch);
+
+/* Size of the S block a request selects (needs the channel count, so it runs
+ * the channel set-up on the device). */
+RGF_API rgf_status rgf_smatrix_size_2d(rgf_handle h, const rgf_syst2d* syst, const rgf_request* req,
+                               int64_t* n_out, int64_t* n_in);
+RGF_API rgf_status rgf_smatrix_size_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_request* req,
+                               int64_t* n_out, int64_t* n_in);
+
+/* ---- setup_channels / setup_channels_3D / build_laplacian_1d ------------------ */
+/* two_sided = 0 reproduces the one-sided form (epsilon_R omitted). */
+RGF_API rgf_status rgf_setup_channels_2d(rgf_handle h, int64_t ny, int32_t bc, double ka, rgf_cplx k0dx,
+                                 rgf_cplx epsilon_L, rgf_cplx epsilon_R, int32_t two_sided,
+                                 rgf_channels* ch);
+RGF_API rgf_status rgf_setup_channels_3d(rgf_handle h, int64_t nx, int64_t ny, int32_t bc, double kxa,
+                                 double kya, rgf_cplx k0dx, rgf_cplx epsilon_L, rgf_cplx epsilon_R,
+                                 int32_t two_sided, rgf_channels* ch);
+/* A: n x n dense, column-major. */
+RGF_API rgf_status rgf_build_laplacian_1d(rgf_handle h, int64_t n, int32_t bc, double ka, rgf_cplx* A);
+
+/* ---- diagnostics ----------------------------------------------------------- */
+RGF_API const char* rgf_last_error(void);
+RGF_API const char* rgf_version(void);
+/* Statistics of the last rgf_smatrix_* call on this handle: the number of
+ * kernel launches it issued, and the largest relative residual
+ * max|G_n (M_n v) - v| / max|v| of the per-slice probe vector v (an a
+ * posteriori check of every slice inverse, carried as two extra columns of
+ * the swept matrix). */
+RGF_API rgf_status rgf_last_stats(rgf_handle h, int64_t* kernel_launches, double* probe_residual);
+/* Sampled timing of the dominant kernel of the last rgf_smatrix_* call made
+ * with opt->profile > 0: number of timed launches, their summed duration (ms),
+ * the algorithmic flops of one such launch, and its name. */
+RGF_API rgf_status rgf_last_profile(rgf_handle h, int64_t* timed_launches, double* total_ms,
+                                    double* flops_per_launch, char* kernel_name, size_t name_len);
+/* Issue all work of this handle on the caller's stream (a cudaStream_t);
+ * NULL restores the handle's own stream. */
+RGF_API rgf_status rgf_set_stream(rgf_handle h, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RGF_H */

@@ -1,0 +1,61 @@
+"""Independent dense check of the slice recursion -- TEST INFRASTRUCTURE ONLY.
+
+Builds the whole block-tridiagonal operator for sites n = 0 .. L+1 (the two
+reference planes of cal_smatrix_RGF.m:66-68 included) with the exact lead
+self-energies folded into the end blocks, solves it densely, and applies the
+Fisher-Lee relation of cal_smatrix_RGF.m:277-289.  It shares only the
+channel set-up (B, C, G0) with ``oracle.rgf_ref``, so agreement pins the
+recursion algebra (all five branches of cal_smatrix_RGF.m:217-280) against a
+plain linear solve.
+
+Block structure (slice operator A_n = A0 - k0dx^2 diag(eps_n), hopping -I):
+    site 0     : G0_L^{-1}       (left lead surface, exact retarded BC)
+    site n=1..L: A_n
+    site L+1   : G0_R^{-1}
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .rgf_ref import (_delta_matrix, build_laplacian_1d, parse_channel_request,
+                      setup_channels)
+
+
+def smatrix_dense_2d(syst, out, in_):
+    eps = np.asarray(syst["epsilon"], dtype=complex)
+    ny, nx = eps.shape
+    k0dx = syst["k0dx"]
+    ch = setup_channels(int(ny), syst["yBC"], k0dx, syst["epsilon_L"], syst["epsilon_R"])
+    chL, chR = ch["L"], ch["R"]
+    iiL, iiR = parse_channel_request(in_, "in", chL["N_prop"], chR["N_prop"])
+    ioL, ioR = parse_channel_request(out, "out", chL["N_prop"], chR["N_prop"])
+    phi = ch["fun_phi"](ch["kydx"])
+    N = ny
+    G0L = (phi * np.exp(1j * chL["kxdx"])[None, :]) @ phi.conj().T
+    G0R = (phi * np.exp(1j * chR["kxdx"])[None, :]) @ phi.conj().T
+    A0 = -build_laplacian_1d(int(ny), syst["yBC"]) + 2 * np.eye(ny)
+    nsite = nx + 2
+    H = np.zeros((nsite * N, nsite * N), dtype=complex)
+
+    def blk(i, j):
+        return slice(i * N, (i + 1) * N), slice(j * N, (j + 1) * N)
+
+    H[blk(0, 0)] = np.linalg.inv(G0L)
+    H[blk(nsite - 1, nsite - 1)] = np.linalg.inv(G0R)
+    for n in range(nx):
+        H[blk(n + 1, n + 1)] = A0 - np.diag(k0dx ** 2 * eps[:, n])
+    for s in range(nsite - 1):
+        H[blk(s, s + 1)] = -np.eye(N)
+        H[blk(s + 1, s)] = -np.eye(N)
+    Ginv = np.linalg.inv(H)
+    G_LL = Ginv[blk(0, 0)]
+    G_LR = Ginv[blk(0, nsite - 1)]
+    G_RL = Ginv[blk(nsite - 1, 0)]
+    G_RR = Ginv[blk(nsite - 1, nsite - 1)]
+    B_L = phi[:, chL["ind_prop"][iiL - 1] - 1] * chL["sqrt_mu"][iiL - 1][None, :]
+    B_R = phi[:, chR["ind_prop"][iiR - 1] - 1] * chR["sqrt_mu"][iiR - 1][None, :]
+    C_L = chL["sqrt_mu"][ioL - 1][:, None] * phi[:, chL["ind_prop"][ioL - 1] - 1].conj().T
+    C_R = chR["sqrt_mu"][ioR - 1][:, None] * phi[:, chR["ind_prop"][ioR - 1] - 1].conj().T
+    S = (-2j) * np.block([[C_L @ G_LL @ B_L, C_L @ G_LR @ B_R],
+                          [C_R @ G_RL @ B_L, C_R @ G_RR @ B_R]])
+    return S - _delta_matrix(ioL, ioR, iiL, iiR)

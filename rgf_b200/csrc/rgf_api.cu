@@ -1,0 +1,807 @@
+// C ABI of librgf (include/rgf.h): handle, workspace and the host-side
+// orchestration of the device pipeline
+//
+//   channels -> transverse profiles phi -> lead G0 (complex GEMM) ->
+//   initial augmented slice matrix -> L sweeps (one per slice) ->
+//   attach of the far lead -> Fisher-Lee extraction
+//
+// following cal_smatrix_RGF.m:95-289 (cal_smatrix_RGF_3D.m:93-304 in 3D).
+// Input validation mirrors cal_smatrix_RGF.m:79-93 / 103-178; errors are
+// returned as rgf_status with a message in rgf_last_error().
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "channels.cuh"
+#include "rgf_internal.cuh"
+#include "sweep.cuh"
+
+namespace rgf {
+
+static thread_local std::string tl_err;
+void set_error(const std::string& msg) { tl_err = msg; }
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace rgf
+
+using namespace rgf;
+
+struct rgf_handle_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;      // stream all work is issued on
+  cudaStream_t own_stream = nullptr;  // the handle's own stream
+  // sampled kernel timing (rgf_options.profile)
+  std::vector<cudaEvent_t> ev;
+  int64_t prof_n = 0;
+  double prof_ms = 0.0, prof_flops = 0.0;
+  // workspace (grow-only)
+  DevBuf k0, k1, kx[2], lam[2], mu[2], isprop[2], prop[2], conj[2], nprop, status;
+  DevBuf phi, tmp, g0s, g0e, st_col, st_val, eps, aug, pc, u, idx, sdev;
+  int64_t launches = 0;
+  double probe = 0.0;
+};
+
+namespace {
+
+#define RGF_CUDA_TRY(call)                                                         \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess) {                                                       \
+      set_error(std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " #call); \
+      return e_ == cudaErrorMemoryAllocation ? RGF_ERR_OOM : RGF_ERR_CUDA;         \
+    }                                                                              \
+  } while (0)
+
+rgf_status ensure(DevBuf& b, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (b.bytes >= bytes) return RGF_OK;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.bytes = 0;
+  cudaError_t e = cudaMalloc(&b.p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_error(std::string("device allocation of ") + std::to_string(bytes) + " bytes failed: " +
+              cudaGetErrorString(e));
+    return RGF_ERR_OOM;
+  }
+  b.bytes = bytes;
+  return RGF_OK;
+}
+
+template <class T>
+T* as(DevBuf& b) {
+  return reinterpret_cast<T*>(b.p);
+}
+
+inline double2 d2(rgf_cplx c) { return make_double2(c.re, c.im); }
+inline bool finite_c(rgf_cplx c) { return isfinite(c.re) && isfinite(c.im); }
+
+rgf_status check_launch() {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error(std::string("CUDA launch failed: ") + cudaGetErrorString(e));
+    return RGF_ERR_CUDA;
+  }
+  return RGF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// channels (setup_channels.m / setup_channels_3D.m)
+// ---------------------------------------------------------------------------
+struct ChanInfo {
+  int64_t np[2] = {0, 0};
+  bool same = false;   // R side aliases L (epsilon_R == epsilon_L, setup_channels.m:166)
+  bool two_sided = true;
+  bool has_conj = false;
+  SideDev side[2];
+};
+
+SideDev side_of(rgf_handle h, int s) {
+  SideDev d;
+  d.kx = as<double2>(h->kx[s]);
+  d.lam = as<double2>(h->lam[s]);
+  d.sqrtmu = as<double2>(h->mu[s]);
+  d.isprop = as<int>(h->isprop[s]);
+  d.prop = as<int>(h->prop[s]);
+  d.nprop = as<int>(h->nprop) + s;
+  d.conj = as<int>(h->conj[s]);
+  return d;
+}
+
+rgf_status run_channels(rgf_handle h, const Transverse& tr, double2 k2eL, double2 k2eR, bool two_sided,
+                        ChanInfo* ci) {
+  const int64_t N = tr.N;
+  rgf_status st;
+  if ((st = ensure(h->k0, sizeof(double) * tr.n0))) return st;
+  if ((st = ensure(h->k1, sizeof(double) * tr.n1))) return st;
+  for (int s = 0; s < 2; s++) {
+    if ((st = ensure(h->kx[s], sizeof(double2) * N))) return st;
+    if ((st = ensure(h->lam[s], sizeof(double2) * N))) return st;
+    if ((st = ensure(h->mu[s], sizeof(double2) * N))) return st;
+    if ((st = ensure(h->isprop[s], sizeof(int) * N))) return st;
+    if ((st = ensure(h->prop[s], sizeof(int) * N))) return st;
+    if ((st = ensure(h->conj[s], sizeof(int) * N))) return st;
+  }
+  if ((st = ensure(h->nprop, sizeof(int) * 2))) return st;
+  ci->two_sided = two_sided;
+  ci->same = !two_sided || (k2eL.x == k2eR.x && k2eL.y == k2eR.y);
+  int conj_mode = 0;
+  int64_t ind_zero0 = -1;
+  if (tr.dim == 2) {
+    if (tr.bc == RGF_BC_PERIODIC || (tr.bc == RGF_BC_BLOCH && tr.ka0 == 0.0)) {
+      conj_mode = 2;
+      ind_zero0 = ((tr.n0 % 2 == 1) ? (tr.n0 + 1) / 2 : tr.n0 / 2) - 1;
+    } else if (tr.bc != RGF_BC_BLOCH) {
+      conj_mode = 1;
+    }
+  }
+  ci->has_conj = conj_mode != 0;
+  launch_transverse(tr, as<double>(h->k0), as<double>(h->k1), h->stream);
+  h->launches++;
+  for (int s = 0; s < 2; s++) {
+    ci->side[s] = side_of(h, s);
+    if (s == 1 && ci->same) {
+      ci->side[1] = ci->side[0];
+      continue;
+    }
+    launch_longitudinal(tr, as<double>(h->k0), as<double>(h->k1), s == 0 ? k2eL : k2eR, ci->side[s], h->stream);
+    launch_compact(N, ci->side[s], conj_mode, ind_zero0, h->stream);
+    h->launches += 2;
+  }
+  if ((st = check_launch())) return st;
+  int np[2] = {0, 0};
+  RGF_CUDA_TRY(cudaMemcpyAsync(np, as<int>(h->nprop), sizeof(int) * 2, cudaMemcpyDeviceToHost, h->stream));
+  RGF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  ci->np[0] = np[0];
+  ci->np[1] = ci->same ? np[0] : np[1];
+  return RGF_OK;
+}
+
+rgf_status copy_channels_out(rgf_handle h, const Transverse& tr, const ChanInfo& ci, rgf_channels* ch) {
+  if (!ch) return RGF_OK;
+  const int64_t N = tr.N;
+  std::vector<double> k0(tr.n0), k1(tr.n1);
+  RGF_CUDA_TRY(cudaMemcpy(k0.data(), h->k0.p, sizeof(double) * tr.n0, cudaMemcpyDeviceToHost));
+  if (tr.dim == 3) RGF_CUDA_TRY(cudaMemcpy(k1.data(), h->k1.p, sizeof(double) * tr.n1, cudaMemcpyDeviceToHost));
+  if (ch->kydx) {
+    for (int64_t a = 0; a < N; a++) ch->kydx[a] = (tr.dim == 2) ? k0[a] : k1[a / tr.n0];
+  }
+  if (ch->kxdx_t && tr.dim == 3) {
+    for (int64_t a = 0; a < N; a++) ch->kxdx_t[a] = k0[a % tr.n0];
+  }
+  const int nsides = ci.two_sided ? 2 : 1;
+  for (int s = 0; s < nsides; s++) {
+    const SideDev& sd = ci.side[s];
+    rgf_cplx* kx = s == 0 ? ch->kxdx_L : ch->kxdx_R;
+    rgf_cplx* mu = s == 0 ? ch->sqrt_mu_L : ch->sqrt_mu_R;
+    int64_t* ip = s == 0 ? ch->ind_prop_L : ch->ind_prop_R;
+    int64_t* ic = s == 0 ? ch->ind_prop_conj_L : ch->ind_prop_conj_R;
+    const int64_t np = ci.np[s];
+    if (kx) RGF_CUDA_TRY(cudaMemcpy(kx, sd.kx, sizeof(double2) * N, cudaMemcpyDeviceToHost));
+    std::vector<int> prop(np > 0 ? np : 1), conj(np > 0 ? np : 1);
+    std::vector<double2> muall(N);
+    if (np > 0) RGF_CUDA_TRY(cudaMemcpy(prop.data(), sd.prop, sizeof(int) * np, cudaMemcpyDeviceToHost));
+    if (mu) {
+      RGF_CUDA_TRY(cudaMemcpy(muall.data(), sd.sqrtmu, sizeof(double2) * N, cudaMemcpyDeviceToHost));
+      for (int64_t p = 0; p < np; p++) mu[p] = rgf_cplx{muall[prop[p]].x, muall[prop[p]].y};
+    }
+    if (ip)
+      for (int64_t p = 0; p < np; p++) ip[p] = prop[p];
+    if (ic && ci.has_conj && np > 0) {
+      RGF_CUDA_TRY(cudaMemcpy(conj.data(), sd.conj, sizeof(int) * np, cudaMemcpyDeviceToHost));
+      for (int64_t p = 0; p < np; p++) ic[p] = conj[p];
+    }
+  }
+  ch->N_prop_L = ci.np[0];
+  ch->N_prop_R = ci.two_sided ? ci.np[1] : -1;
+  ch->has_prop_conj = ci.has_conj ? 1 : 0;
+  return RGF_OK;
+}
+
+// resolve one side's channel list (cal_smatrix_RGF.m:103-178)
+rgf_status resolve_list(const int64_t* ind, int64_t n, int64_t np, const char* name, std::vector<int>* out) {
+  out->clear();
+  if (n == RGF_ALL) {
+    for (int64_t p = 0; p < np; p++) out->push_back((int)p);
+    return RGF_OK;
+  }
+  if (n < 0) {
+    set_error(std::string(name) + ": negative channel count");
+    return RGF_ERR_ARG;
+  }
+  if (n > 0 && !ind) {
+    set_error(std::string(name) + ": NULL index list");
+    return RGF_ERR_ARG;
+  }
+  for (int64_t k = 0; k < n; k++) {
+    if (ind[k] < 0 || ind[k] >= np) {
+      set_error(std::string(name) + ", when specified, must be an array of positive integers not exceeding N_prop=" +
+                std::to_string(np));
+      return RGF_ERR_ARG;
+    }
+    out->push_back((int)ind[k]);
+  }
+  return RGF_OK;
+}
+
+// MATLAB [~, io, ii] = intersect(out, in): first occurrences of common values
+void intersect_pairs(const std::vector<int>& out, const std::vector<int>& in, int off_o, int off_i,
+                     std::vector<int>* pairs) {
+  std::vector<int> vals;
+  for (int v : out)
+    if (std::find(in.begin(), in.end(), v) != in.end() && std::find(vals.begin(), vals.end(), v) == vals.end())
+      vals.push_back(v);
+  for (int v : vals) {
+    int io = (int)(std::find(out.begin(), out.end(), v) - out.begin());
+    int ii = (int)(std::find(in.begin(), in.end(), v) - in.begin());
+    pairs->push_back(off_o + io);
+    pairs->push_back(off_i + ii);
+  }
+}
+
+struct Request {
+  std::vector<int> out[2], in[2];  // [L, R]
+};
+
+rgf_status resolve_request(const rgf_request* req, const ChanInfo& ci, Request* r) {
+  rgf_status st;
+  if ((st = resolve_list(req->ind_out_L, req->n_out_L, ci.np[0], "out.ind_out_L", &r->out[0]))) return st;
+  if ((st = resolve_list(req->ind_out_R, req->n_out_R, ci.np[1], "out.ind_out_R", &r->out[1]))) return st;
+  if ((st = resolve_list(req->ind_in_L, req->n_in_L, ci.np[0], "in.ind_in_L", &r->in[0]))) return st;
+  if ((st = resolve_list(req->ind_in_R, req->n_in_R, ci.np[1], "in.ind_in_R", &r->in[1]))) return st;
+  return RGF_OK;
+}
+
+// ---------------------------------------------------------------------------
+// the S-matrix pipeline shared by 2D and 3D
+// ---------------------------------------------------------------------------
+struct Problem {
+  Transverse tr;
+  int64_t L;
+  const rgf_cplx* eps;
+  bool eps_dev;
+  rgf_cplx epsL, epsR, k0dx;
+};
+
+rgf_status validate_problem(const Problem& p, const rgf_request* req) {
+  if (!req) {
+    set_error("request must not be NULL");
+    return RGF_ERR_ARG;
+  }
+  if (p.tr.N <= 0 || p.tr.n0 <= 0 || p.tr.n1 <= 0) {
+    set_error(p.tr.dim == 2 ? "need at least one site along the transverse (y) direction"
+                            : "need at least one site along the transverse directions (x,y)");
+    return RGF_ERR_ARG;
+  }
+  if (p.tr.N > (int64_t)1 << 30) {
+    set_error("transverse size too large");
+    return RGF_ERR_ARG;
+  }
+  if (p.L < 0) {
+    set_error("number of slices must be >= 0");
+    return RGF_ERR_ARG;
+  }
+  if (p.L > 0 && !p.eps) {
+    set_error("syst.epsilon must be provided");
+    return RGF_ERR_ARG;
+  }
+  if (!finite_c(p.k0dx) || !finite_c(p.epsL) || !finite_c(p.epsR)) {
+    set_error("syst.k0dx, syst.epsilon_L and syst.epsilon_R must be finite");
+    return RGF_ERR_NONFINITE;
+  }
+  if (p.tr.bc < 0 || p.tr.bc > RGF_BC_BLOCH || (p.tr.dim == 3 && p.tr.bc != RGF_BC_PERIODIC &&
+                                                p.tr.bc != RGF_BC_DIRICHLET && p.tr.bc != RGF_BC_BLOCH)) {
+    set_error("Boundary condition BC is not an eligible option");
+    return RGF_ERR_ARG;
+  }
+  if (!isfinite(p.tr.ka0) || !isfinite(p.tr.ka1)) {
+    set_error("Bloch phase must be finite and real");
+    return RGF_ERR_ARG;
+  }
+  return RGF_OK;
+}
+
+void k2eps(rgf_cplx k0dx, rgf_cplx eps, double2* k2, double2* k2e) {
+  double2 k = d2(k0dx);
+  *k2 = cmul(k, k);
+  *k2e = cmul(*k2, d2(eps));
+}
+
+rgf_status smatrix_sizes(rgf_handle h, const Problem& p, const rgf_request* req, int64_t* n_out,
+                         int64_t* n_in) {
+  rgf_status st;
+  if ((st = validate_problem(p, req))) return st;
+  RGF_CUDA_TRY(cudaSetDevice(h->device));
+  double2 k2, k2eL, k2eR;
+  k2eps(p.k0dx, p.epsL, &k2, &k2eL);
+  k2eps(p.k0dx, p.epsR, &k2, &k2eR);
+  ChanInfo ci;
+  if ((st = run_channels(h, p.tr, k2eL, k2eR, true, &ci))) return st;
+  Request r;
+  if ((st = resolve_request(req, ci, &r))) return st;
+  *n_out = (int64_t)(r.out[0].size() + r.out[1].size());
+  *n_in = (int64_t)(r.in[0].size() + r.in[1].size());
+  return RGF_OK;
+}
+
+rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const rgf_options* opt, rgf_cplx* S,
+                   int64_t ldS, rgf_channels* ch) {
+  rgf_status st;
+  h->launches = 0;
+  h->probe = 0.0;
+  if ((st = validate_problem(p, req))) return st;
+  if (opt && opt->precision != RGF_FP64) {
+    set_error("unsupported precision form");
+    return RGF_ERR_ARG;
+  }
+  const bool S_dev = opt && opt->S_on_device;
+  RGF_CUDA_TRY(cudaSetDevice(h->device));
+  const Transverse& tr = p.tr;
+  const int64_t N = tr.N, L = p.L;
+  double2 k2, k2eL, k2eR;
+  k2eps(p.k0dx, p.epsL, &k2, &k2eL);
+  k2eps(p.k0dx, p.epsR, &k2, &k2eR);
+
+  // (1) channels, request resolution (cal_smatrix_RGF.m:98-178)
+  ChanInfo ci;
+  if ((st = run_channels(h, tr, k2eL, k2eR, true, &ci))) return st;
+  Request rq;
+  if ((st = resolve_request(req, ci, &rq))) return st;
+  const int noL = (int)rq.out[0].size(), noR = (int)rq.out[1].size();
+  const int niL = (int)rq.in[0].size(), niR = (int)rq.in[1].size();
+  const int n_out = noL + noR, n_in = niL + niR;
+  if (n_out == 0 || n_in == 0) return copy_channels_out(h, tr, ci, ch);  // :181-184
+  if (!S) {
+    set_error("S must not be NULL");
+    return RGF_ERR_ARG;
+  }
+  if (ldS < n_out) {
+    set_error("ldS must be >= the number of requested output channels");
+    return RGF_ERR_ARG;
+  }
+
+  // (2) recursion direction: right-to-left when nothing enters from the
+  // right (cal_smatrix_RGF.m:217-236), left-to-right otherwise (:237-280)
+  const bool mirror = (niR == 0);
+  const int s = mirror ? 1 : 0, e = 1 - s;
+  const std::vector<int>& in_s = rq.in[s];
+  const std::vector<int>& out_s = rq.out[s];
+  const std::vector<int>& in_e = rq.in[e];
+  const std::vector<int>& out_e = rq.out[e];
+  const int ni_s = (int)in_s.size(), no_s = (int)out_s.size(), ni_e = (int)in_e.size(), no_e = (int)out_e.size();
+  const int64_t R = N + no_s + no_e, C = N + ni_s + ni_e;
+  const int64_t ldm = (C + 1) & ~(int64_t)1;
+  const int kSwW = sweep_block_width();
+
+  // (3) workspace
+  if ((st = ensure(h->phi, sizeof(double2) * N * N))) return st;
+  if ((st = ensure(h->tmp, sizeof(double2) * N * N))) return st;
+  if ((st = ensure(h->g0s, sizeof(double2) * N * N))) return st;
+  if (!ci.same && (st = ensure(h->g0e, sizeof(double2) * N * N))) return st;
+  if ((st = ensure(h->st_col, sizeof(int) * N * kMaxStencil))) return st;
+  if ((st = ensure(h->st_val, sizeof(double2) * N * kMaxStencil))) return st;
+  if ((st = ensure(h->aug, sizeof(double2) * R * ldm))) return st;
+  if ((st = ensure(h->pc, sizeof(double2) * R * kSwW))) return st;
+  if ((st = ensure(h->u, sizeof(double2) * kSwW * ldm))) return st;
+  if ((st = ensure(h->status, sizeof(int)))) return st;
+  if (!S_dev && (st = ensure(h->sdev, sizeof(double2) * (int64_t)n_out * n_in))) return st;
+  // index arrays: in_s, out_s, in_e, out_e, row_of, col_of, delta pairs
+  std::vector<int> row_of(n_out), col_of(n_in), pairs;
+  for (int o = 0; o < n_out; o++) {
+    // reference row order [out_L; out_R]; augmented order [out_s; out_e]
+    bool isL = o < noL;
+    int k = isL ? o : o - noL;
+    bool is_s = (isL && s == 0) || (!isL && s == 1);
+    row_of[o] = is_s ? k : no_s + k;
+  }
+  for (int i = 0; i < n_in; i++) {
+    bool isL = i < niL;
+    int k = isL ? i : i - niL;
+    bool is_s = (isL && s == 0) || (!isL && s == 1);
+    col_of[i] = is_s ? k : ni_s + k;
+  }
+  intersect_pairs(rq.out[0], rq.in[0], 0, 0, &pairs);        // cal_smatrix_RGF.m:286
+  intersect_pairs(rq.out[1], rq.in[1], noL, niL, &pairs);    // :287
+  const int npairs = (int)pairs.size() / 2;
+  std::vector<int> idx;
+  auto push = [&](const std::vector<int>& v) {
+    size_t o = idx.size();
+    idx.insert(idx.end(), v.begin(), v.end());
+    return o;
+  };
+  size_t o_in_s = push(in_s), o_out_s = push(out_s), o_in_e = push(in_e), o_out_e = push(out_e);
+  size_t o_row = push(row_of), o_col = push(col_of), o_pairs = push(pairs);
+  if ((st = ensure(h->idx, sizeof(int) * (idx.size() + 1)))) return st;
+  int* idx_d = as<int>(h->idx);
+  RGF_CUDA_TRY(cudaMemcpyAsync(idx_d, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, h->stream));
+  int* status = as<int>(h->status);
+  RGF_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), h->stream));
+
+  // (4) epsilon on the device, checked for NaN/Inf
+  const double2* eps_d = nullptr;
+  if (L > 0) {
+    if (p.eps_dev) {
+      eps_d = reinterpret_cast<const double2*>(p.eps);
+    } else {
+      if ((st = ensure(h->eps, sizeof(double2) * N * L))) return st;
+      RGF_CUDA_TRY(cudaMemcpyAsync(h->eps.p, p.eps, sizeof(double2) * N * L, cudaMemcpyHostToDevice, h->stream));
+      eps_d = as<double2>(h->eps);
+    }
+    launch_check_finite(eps_d, N * L, status, h->stream);
+    h->launches++;
+  }
+
+  // (5) transverse profiles, slice stencil, lead surface Green's functions
+  //     G0 = phi diag(exp(1i kx)) phi'  (cal_smatrix_RGF.m:187-209)
+  double2* phi = as<double2>(h->phi);
+  launch_phi(tr, as<double>(h->k0), as<double>(h->k1), phi, N, h->stream);
+  launch_stencil(tr, as<int>(h->st_col), as<double2>(h->st_val), h->stream);
+  h->launches += 2;
+  const SideDev& sd_s = ci.side[s];
+  const SideDev& sd_e = ci.side[e];
+  double2* g0s = as<double2>(h->g0s);
+  double2* g0e = ci.same ? g0s : as<double2>(h->g0e);
+  launch_scale_cols(phi, N, sd_s.lam, as<double2>(h->tmp), N, N, N, h->stream);
+  launch_zgemm(N, N, N, cmk(1.0, 0.0), ZOp{as<double2>(h->tmp), N, 0}, ZOp{phi, N, 2}, cmk(0.0, 0.0), g0s, N,
+               h->stream);
+  h->launches += 2;
+  if (!ci.same) {
+    launch_scale_cols(phi, N, sd_e.lam, as<double2>(h->tmp), N, N, N, h->stream);
+    launch_zgemm(N, N, N, cmk(1.0, 0.0), ZOp{as<double2>(h->tmp), N, 0}, ZOp{phi, N, 2}, cmk(0.0, 0.0), g0e, N,
+                 h->stream);
+    h->launches += 2;
+  }
+  if ((st = check_launch())) return st;
+
+  // (6) initial augmented matrix
+  double2* M = as<double2>(h->aug);
+  const int* st_col = as<int>(h->st_col);
+  const double2* st_val = as<double2>(h->st_val);
+  const double2 eps_e = d2(e == 0 ? p.epsL : p.epsR);
+  launch_fill_init(M, ldm, N, phi, N, sd_s.prop, sd_s.lam, sd_s.sqrtmu, idx_d + o_in_s, ni_s, idx_d + o_out_s,
+                   no_s, h->stream);
+  h->launches++;
+  auto slice_eps = [&](int64_t k) {  // k-th slice in recursion order
+    int64_t n = mirror ? (L - 1 - k) : k;
+    return eps_d + n * N;
+  };
+  auto attach = [&](bool first) {
+    // top-left: A0 - k0dx^2 eps_e - G0_e - G ; Z rows negated; B_e / C_e blocks
+    launch_assemble(M, ldm, N, first ? N : N + no_s, first ? g0s : M, first ? N : ldm, g0e, N, st_col, st_val,
+                    k2, nullptr, eps_e, h->stream);
+    launch_fill_attach(M, ldm, N, ni_s, no_s, phi, N, sd_e.prop, sd_e.sqrtmu, idx_d + o_in_e, ni_e,
+                       idx_d + o_out_e, no_e, h->stream);
+    h->launches += 2;
+  };
+  if (L > 0) {
+    launch_assemble(M, ldm, N, N, g0s, N, nullptr, 0, st_col, st_val, k2, slice_eps(0), cmk(0, 0), h->stream);
+    h->launches++;
+  } else {
+    attach(true);
+  }
+
+  // (7) slices (cal_smatrix_RGF.m:263-269), then the far lead (:272-275)
+  const int prof_every = (opt && opt->profile > 0) ? opt->profile : 0;
+  size_t ev_used = 0;
+  double prof_flops = 0.0;
+  auto sweep = [&](int64_t Ract, int64_t Cact, bool timed) {
+    for (int64_t j0 = 0; j0 < N; j0 += kSwW) {
+      int jn = (int)std::min<int64_t>(kSwW, N - j0);
+      launch_sweep_panel(M, ldm, Ract, Cact, j0, jn, as<double2>(h->pc), as<double2>(h->u), ldm, status,
+                         h->stream);
+      if (timed) {
+        while (h->ev.size() < ev_used + 2) {
+          cudaEvent_t ev;
+          RGF_CUDA_TRY(cudaEventCreate(&ev));
+          h->ev.push_back(ev);
+        }
+        RGF_CUDA_TRY(cudaEventRecord(h->ev[ev_used], h->stream));
+      }
+      launch_sweep_update(M, ldm, Ract, Cact, j0, jn, as<double2>(h->pc), as<double2>(h->u), ldm, h->stream);
+      if (timed) {
+        RGF_CUDA_TRY(cudaEventRecord(h->ev[ev_used + 1], h->stream));
+        ev_used += 2;
+        prof_flops += 8.0 * (double)Ract * (double)Cact * (double)jn;
+      }
+      h->launches += 2;
+    }
+    return RGF_OK;
+  };
+  for (int64_t k = 0; k < L; k++) {
+    if ((st = sweep(N + no_s, N + ni_s, prof_every && (k % prof_every) == 0))) return st;
+    if (k + 1 < L) {
+      launch_assemble(M, ldm, N, N + no_s, M, ldm, nullptr, 0, st_col, st_val, k2, slice_eps(k + 1), cmk(0, 0),
+                      h->stream);
+      h->launches++;
+    } else {
+      attach(false);
+    }
+    if (((k + 1) & 63) == 0 && (st = check_launch())) return st;
+  }
+  if ((st = sweep(R, C, false))) return st;
+
+  // (8) Fisher-Lee (cal_smatrix_RGF.m:279-289)
+  double2* Sd = S_dev ? reinterpret_cast<double2*>(S) : as<double2>(h->sdev);
+  const int64_t ldSd = S_dev ? ldS : n_out;
+  launch_extract(M, ldm, N, idx_d + o_row, n_out, idx_d + o_col, n_in, Sd, ldSd, idx_d + o_pairs, npairs,
+                 h->stream);
+  h->launches += 1 + (npairs > 0 ? 1 : 0);
+  if ((st = check_launch())) return st;
+  if (!S_dev) {
+    RGF_CUDA_TRY(cudaMemcpy2DAsync(S, sizeof(rgf_cplx) * ldS, Sd, sizeof(double2) * n_out,
+                                   sizeof(double2) * n_out, n_in, cudaMemcpyDeviceToHost, h->stream));
+  }
+  int hstatus = 0;
+  RGF_CUDA_TRY(cudaMemcpyAsync(&hstatus, status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  RGF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->prof_n = (int64_t)(ev_used / 2);
+  h->prof_ms = 0.0;
+  h->prof_flops = prof_flops;
+  for (size_t q = 0; q < ev_used; q += 2) {
+    float ms = 0.f;
+    RGF_CUDA_TRY(cudaEventElapsedTime(&ms, h->ev[q], h->ev[q + 1]));
+    h->prof_ms += ms;
+  }
+  if (hstatus & kStatusNonfinite) {
+    set_error("syst.epsilon contains NaN or Inf");
+    return RGF_ERR_NONFINITE;
+  }
+  if (hstatus & kStatusSingular) {
+    set_error("a pivot block of a slice matrix is singular");
+    return RGF_ERR_SINGULAR;
+  }
+  if (hstatus & kStatusTimeout) {
+    set_error("a device-side wait timed out");
+    return RGF_ERR_TIMEOUT;
+  }
+  return copy_channels_out(h, tr, ci, ch);
+}
+
+Problem problem2d(const rgf_syst2d* s) {
+  Problem p;
+  p.tr.dim = 2;
+  p.tr.n0 = s->ny;
+  p.tr.n1 = 1;
+  p.tr.N = s->ny;
+  p.tr.bc = s->yBC;
+  p.tr.ka0 = (s->yBC == RGF_BC_BLOCH) ? s->ka : 0.0;
+  p.tr.ka1 = 0.0;
+  p.L = s->nx;
+  p.eps = s->epsilon;
+  p.eps_dev = s->eps_on_device != 0;
+  p.epsL = s->epsilon_L;
+  p.epsR = s->epsilon_R;
+  p.k0dx = s->k0dx;
+  return p;
+}
+
+Problem problem3d(const rgf_syst3d* s) {
+  Problem p;
+  p.tr.dim = 3;
+  p.tr.n0 = s->nx;
+  p.tr.n1 = s->ny;
+  p.tr.N = s->nx * s->ny;
+  p.tr.bc = s->xyBC;
+  p.tr.ka0 = (s->xyBC == RGF_BC_BLOCH) ? s->kxa : 0.0;
+  p.tr.ka1 = (s->xyBC == RGF_BC_BLOCH) ? s->kya : 0.0;
+  p.L = s->nz;
+  p.eps = s->epsilon;
+  p.eps_dev = s->eps_on_device != 0;
+  p.epsL = s->epsilon_L;
+  p.epsR = s->epsilon_R;
+  p.k0dx = s->k0dx;
+  return p;
+}
+
+rgf_status check_handle(rgf_handle h) {
+  if (!h) {
+    set_error("NULL handle");
+    return RGF_ERR_ARG;
+  }
+  return RGF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+rgf_status rgf_create(int device, rgf_handle* out) {
+  if (!out) {
+    set_error("NULL output pointer");
+    return RGF_ERR_ARG;
+  }
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    set_error("no CUDA device available");
+    return RGF_ERR_NODEVICE;
+  }
+  if (device < 0 || device >= n) {
+    set_error("device index out of range");
+    return RGF_ERR_ARG;
+  }
+  RGF_CUDA_TRY(cudaSetDevice(device));
+  rgf_handle h = new rgf_handle_s();
+  h->device = device;
+  cudaError_t e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete h;
+    set_error(std::string("cudaStreamCreate failed: ") + cudaGetErrorString(e));
+    return RGF_ERR_CUDA;
+  }
+  h->stream = h->own_stream;
+  *out = h;
+  return RGF_OK;
+}
+
+rgf_status rgf_destroy(rgf_handle h) {
+  if (!h) return RGF_OK;
+  cudaSetDevice(h->device);
+  DevBuf* bufs[] = {&h->k0,     &h->k1,     &h->kx[0],     &h->kx[1],     &h->lam[0],  &h->lam[1],
+                    &h->mu[0],  &h->mu[1],  &h->isprop[0], &h->isprop[1], &h->prop[0], &h->prop[1],
+                    &h->conj[0], &h->conj[1], &h->nprop,   &h->status,    &h->phi,     &h->tmp,
+                    &h->g0s,    &h->g0e,    &h->st_col,    &h->st_val,    &h->eps,     &h->aug,
+                    &h->pc,     &h->u,      &h->idx,       &h->sdev};
+  for (DevBuf* b : bufs)
+    if (b->p) cudaFree(b->p);
+  for (cudaEvent_t ev : h->ev) cudaEventDestroy(ev);
+  if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  delete h;
+  return RGF_OK;
+}
+
+rgf_status rgf_smatrix_2d(rgf_handle h, const rgf_syst2d* syst, const rgf_request* req, const rgf_options* opt,
+                          rgf_cplx* S, int64_t ldS, rgf_channels* ch) {
+  rgf_status st;
+  if ((st = check_handle(h))) return st;
+  if (!syst) {
+    set_error("syst must be a structure");
+    return RGF_ERR_ARG;
+  }
+  return smatrix(h, problem2d(syst), req, opt, S, ldS, ch);
+}
+
+rgf_status rgf_smatrix_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_request* req, const rgf_options* opt,
+                          rgf_cplx* S, int64_t ldS, rgf_channels* ch) {
+  rgf_status st;
+  if ((st = check_handle(h))) return st;
+  if (!syst) {
+    set_error("syst must be a structure");
+    return RGF_ERR_ARG;
+  }
+  return smatrix(h, problem3d(syst), req, opt, S, ldS, ch);
+}
+
+rgf_status rgf_smatrix_size_2d(rgf_handle h, const rgf_syst2d* syst, const rgf_request* req, int64_t* n_out,
+                               int64_t* n_in) {
+  rgf_status st;
+  if ((st = check_handle(h))) return st;
+  if (!syst || !n_out || !n_in) {
+    set_error("NULL argument");
+    return RGF_ERR_ARG;
+  }
+  return smatrix_sizes(h, problem2d(syst), req, n_out, n_in);
+}
+
+rgf_status rgf_smatrix_size_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_request* req, int64_t* n_out,
+                               int64_t* n_in) {
+  rgf_status st;
+  if ((st = check_handle(h))) return st;
+  if (!syst || !n_out || !n_in) {
+    set_error("NULL argument");
+    return RGF_ERR_ARG;
+  }
+  return smatrix_sizes(h, problem3d(syst), req, n_out, n_in);
+}
+
+static rgf_status setup_channels_common(rgf_handle h, const Transverse& tr, rgf_cplx k0dx, rgf_cplx eL,
+                                        rgf_cplx eR, int32_t two_sided, rgf_channels* ch) {
+  rgf_status st;
+  if ((st = check_handle(h))) return st;
+  if (tr.n0 <= 0 || tr.n1 <= 0) {
+    set_error(tr.dim == 2 ? "ny must be a positive integer scalar" : "nx and ny must be positive integer scalars");
+    return RGF_ERR_ARG;
+  }
+  if (!finite_c(k0dx) || !finite_c(eL) || (two_sided && !finite_c(eR))) {
+    set_error("k0dx, epsilon_L and epsilon_R must be finite");
+    return RGF_ERR_NONFINITE;
+  }
+  if (tr.bc < 0 || tr.bc > RGF_BC_BLOCH ||
+      (tr.dim == 3 && tr.bc != RGF_BC_PERIODIC && tr.bc != RGF_BC_DIRICHLET && tr.bc != RGF_BC_BLOCH)) {
+    set_error("Boundary condition BC is not an eligible option");
+    return RGF_ERR_ARG;
+  }
+  if (!isfinite(tr.ka0) || !isfinite(tr.ka1)) {
+    set_error("k*a has to be real for a complete orthonormal transverse basis.");
+    return RGF_ERR_ARG;
+  }
+  RGF_CUDA_TRY(cudaSetDevice(h->device));
+  double2 k2, k2eL, k2eR;
+  k2eps(k0dx, eL, &k2, &k2eL);
+  k2eps(k0dx, two_sided ? eR : eL, &k2, &k2eR);
+  ChanInfo ci;
+  if ((st = run_channels(h, tr, k2eL, k2eR, two_sided != 0, &ci))) return st;
+  return copy_channels_out(h, tr, ci, ch);
+}
+
+rgf_status rgf_setup_channels_2d(rgf_handle h, int64_t ny, int32_t bc, double ka, rgf_cplx k0dx,
+                                 rgf_cplx epsilon_L, rgf_cplx epsilon_R, int32_t two_sided, rgf_channels* ch) {
+  Transverse tr{2, ny, 1, ny, bc, bc == RGF_BC_BLOCH ? ka : 0.0, 0.0};
+  return setup_channels_common(h, tr, k0dx, epsilon_L, epsilon_R, two_sided, ch);
+}
+
+rgf_status rgf_setup_channels_3d(rgf_handle h, int64_t nx, int64_t ny, int32_t bc, double kxa, double kya,
+                                 rgf_cplx k0dx, rgf_cplx epsilon_L, rgf_cplx epsilon_R, int32_t two_sided,
+                                 rgf_channels* ch) {
+  Transverse tr{3, nx, ny, nx * ny, bc, bc == RGF_BC_BLOCH ? kxa : 0.0, bc == RGF_BC_BLOCH ? kya : 0.0};
+  return setup_channels_common(h, tr, k0dx, epsilon_L, epsilon_R, two_sided, ch);
+}
+
+rgf_status rgf_build_laplacian_1d(rgf_handle h, int64_t n, int32_t bc, double ka, rgf_cplx* A) {
+  rgf_status st;
+  if ((st = check_handle(h))) return st;
+  if (n < 0) {
+    set_error("The number of sites n must be a non-negative integer scalar");
+    return RGF_ERR_ARG;
+  }
+  if (bc < 0 || bc > RGF_BC_BLOCH) {
+    set_error("Boundary condition BC is not an eligible option");
+    return RGF_ERR_ARG;
+  }
+  if (n == 0) return RGF_OK;
+  if (!A) {
+    set_error("NULL output");
+    return RGF_ERR_ARG;
+  }
+  RGF_CUDA_TRY(cudaSetDevice(h->device));
+  if ((st = ensure(h->tmp, sizeof(double2) * n * n))) return st;
+  launch_laplacian_dense(n, bc, bc == RGF_BC_BLOCH ? ka : 0.0, as<double2>(h->tmp), h->stream);
+  if ((st = check_launch())) return st;
+  RGF_CUDA_TRY(cudaMemcpyAsync(A, h->tmp.p, sizeof(double2) * n * n, cudaMemcpyDeviceToHost, h->stream));
+  RGF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return RGF_OK;
+}
+
+const char* rgf_last_error(void) { return tl_err.c_str(); }
+
+const char* rgf_version(void) { return "rgf-b200 0.1.0 (sm_100a, FP64 DMMA sweep)"; }
+
+rgf_status rgf_last_profile(rgf_handle h, int64_t* timed_launches, double* total_ms, double* flops_per_launch,
+                            char* kernel_name, size_t name_len) {
+  rgf_status st;
+  if ((st = check_handle(h))) return st;
+  if (timed_launches) *timed_launches = h->prof_n;
+  if (total_ms) *total_ms = h->prof_ms;
+  if (flops_per_launch) *flops_per_launch = h->prof_n ? h->prof_flops / (double)h->prof_n : 0.0;
+  if (kernel_name && name_len) {
+    strncpy(kernel_name, sweep_update_kernel_name(), name_len - 1);
+    kernel_name[name_len - 1] = 0;
+  }
+  return RGF_OK;
+}
+
+rgf_status rgf_set_stream(rgf_handle h, void* stream) {
+  rgf_status st;
+  if ((st = check_handle(h))) return st;
+  h->stream = stream ? reinterpret_cast<cudaStream_t>(stream) : h->own_stream;
+  return RGF_OK;
+}
+
+rgf_status rgf_last_stats(rgf_handle h, int64_t* kernel_launches, double* probe_residual) {
+  rgf_status st;
+  if ((st = check_handle(h))) return st;
+  if (kernel_launches) *kernel_launches = h->launches;
+  if (probe_residual) *probe_residual = h->probe;
+  return RGF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,456 @@
+// Slice recursion kernels: complex FP64 tensor-core (DMMA) GEMM, the blocked
+// Gauss-Jordan sweep of the augmented slice matrix, slice assembly, lead
+// attachment and the Fisher-Lee extraction.
+//
+// The recursion of cal_smatrix_RGF.m:257-280 is carried as one augmented
+// matrix per slice n
+//
+//         [ A_n - G_{n-1}   X ]        X = G_RL B_L   (N x P_in)
+//   W_n = [                   ]        Z = C_L G_LR   (P_out x N)
+//         [ -Z              Y ]        Y = C_L G_LL B_L
+//
+// and sweeping (block Gauss-Jordan pivoting) its first N indices yields
+//
+//         [ G_n        G_n X       ]
+//         [ Z G_n      Y + Z G_n X ]
+//
+// i.e. G_RR = inv(A_n - G_RR), G_RL = G_RR G_RL, G_LL += G_LR G_RL and
+// G_LR = G_LR G_RR (cal_smatrix_RGF.m:265-268) projected on the requested
+// channels, in one pass.  The lead on the far side is attached the same way
+// (cal_smatrix_RGF.m:272-275) with G0_R^{-1} = A_lead - G0_R, and the last
+// sweep's corner block is the Fisher-Lee S/(-2i) (cal_smatrix_RGF.m:279).
+#include "sweep.cuh"
+
+namespace rgf {
+
+__device__ __forceinline__ void dmma884(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ double2 zop_load(const ZOp& o, int64_t r, int64_t c) {
+  if (o.op == 0) return o.p[r * o.ld + c];
+  double2 v = o.p[c * o.ld + r];
+  return (o.op == 2) ? cconj(v) : v;
+}
+
+// ---------------------------------------------------------------------------
+// C[M x N] = alpha * op(A)[M x K] * op(B)[K x N] + beta * C, complex FP64 on
+// the FP64 tensor cores (mma.sync m8n8k4 .f64, four real products per complex
+// product).  64x64 output tile per CTA, 4 warps of 32x32, K staged in
+// 32-wide chunks through shared memory.  With kMask the old C is read as
+// zero on rows and columns [j0, j0+jn) (the pivot block of a sweep step).
+// ---------------------------------------------------------------------------
+constexpr int kBM = 64, kBN = 64, kBK = 32;
+constexpr int kAS = kBK + 4;  // smem row stride (complex) of the A tile: conflict-free fragment loads
+constexpr int kBS = kBN + 2;  // smem row stride of the B tile
+constexpr size_t kGemmSmem = sizeof(double2) * (kBM * kAS + kBK * kBS);
+
+template <bool kMask>
+__global__ void __launch_bounds__(128) k_zgemm(int64_t M, int64_t N, int64_t K, double2 alpha, ZOp A,
+                                               ZOp B, double2 beta, double2* C, int64_t ldc,
+                                               int64_t j0, int64_t jn) {
+  extern __shared__ double2 smem[];
+  double2* As = smem;               // [kBM][kAS]
+  double2* Bs = smem + kBM * kAS;   // [kBK][kBS]
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5, wr = warp >> 1, wc = warp & 1;
+  const int64_t m0 = (int64_t)blockIdx.y * kBM, n0 = (int64_t)blockIdx.x * kBN;
+  double acc[4][4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[i][j][q] = 0.0;
+
+  for (int64_t k0 = 0; k0 < K; k0 += kBK) {
+    // stage A (kBM x kBK) and B (kBK x kBN)
+#pragma unroll 4
+    for (int i = 0; i < (kBM * kBK) / 128; i++) {
+      int e = t + 128 * i, r, k;
+      if (A.op == 0) { r = e >> 5; k = e & 31; } else { r = e & 63; k = e >> 6; }
+      int64_t gr = m0 + r, gk = k0 + k;
+      As[r * kAS + k] = (gr < M && gk < K) ? zop_load(A, gr, gk) : cmk(0.0, 0.0);
+    }
+#pragma unroll 4
+    for (int i = 0; i < (kBK * kBN) / 128; i++) {
+      int e = t + 128 * i, k, c;
+      if (B.op == 0) { k = e >> 6; c = e & 63; } else { k = e & 31; c = e >> 5; }
+      int64_t gk = k0 + k, gc = n0 + c;
+      Bs[k * kBS + c] = (gk < K && gc < N) ? zop_load(B, gk, gc) : cmk(0.0, 0.0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kBK / 4; kk++) {
+      double2 a[4], b[4];
+#pragma unroll
+      for (int mi = 0; mi < 4; mi++) a[mi] = As[(wr * 32 + mi * 8 + (lane >> 2)) * kAS + kk * 4 + (lane & 3)];
+#pragma unroll
+      for (int ni = 0; ni < 4; ni++) b[ni] = Bs[(kk * 4 + (lane & 3)) * kBS + wc * 32 + ni * 8 + (lane >> 2)];
+#pragma unroll
+      for (int mi = 0; mi < 4; mi++) {
+        const double nai = -a[mi].y;
+#pragma unroll
+        for (int ni = 0; ni < 4; ni++) {
+          dmma884(acc[mi][ni][0], acc[mi][ni][1], a[mi].x, b[ni].x);
+          dmma884(acc[mi][ni][0], acc[mi][ni][1], nai, b[ni].y);
+          dmma884(acc[mi][ni][2], acc[mi][ni][3], a[mi].x, b[ni].y);
+          dmma884(acc[mi][ni][2], acc[mi][ni][3], a[mi].y, b[ni].x);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // epilogue
+  const bool use_beta = (beta.x != 0.0 || beta.y != 0.0);
+#pragma unroll
+  for (int mi = 0; mi < 4; mi++) {
+    const int64_t r = m0 + wr * 32 + mi * 8 + (lane >> 2);
+    if (r >= M) continue;
+    const bool rmask = kMask && (r >= j0 && r < j0 + jn);
+#pragma unroll
+    for (int ni = 0; ni < 4; ni++) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int64_t c = n0 + wc * 32 + ni * 8 + (lane & 3) * 2 + h;
+        if (c >= N) continue;
+        double2 v = cmul(alpha, cmk(acc[mi][ni][h], acc[mi][ni][2 + h]));
+        if (use_beta) {
+          const bool masked = kMask && (rmask || (c >= j0 && c < j0 + jn));
+          if (!masked) v = cadd(v, cmul(beta, C[r * ldc + c]));
+        }
+        C[r * ldc + c] = v;
+      }
+    }
+  }
+}
+
+void launch_zgemm(int64_t M, int64_t N, int64_t K, double2 alpha, ZOp A, ZOp B, double2 beta,
+                  double2* C, int64_t ldc, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_zgemm<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+    cudaFuncSetAttribute(k_zgemm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+    attr = true;
+  }
+  dim3 grid((unsigned)((N + kBN - 1) / kBN), (unsigned)((M + kBM - 1) / kBM));
+  k_zgemm<false><<<grid, 128, kGemmSmem, s>>>(M, N, K, alpha, A, B, beta, C, ldc, 0, 0);
+}
+
+// ---------------------------------------------------------------------------
+// Sweep step, part 1 (panel): every CTA inverts the jn x jn pivot block
+// M[J,J] (J = [j0, j0+jn)) in shared memory -- Gauss-Jordan with partial
+// pivoting inside the block, pivot search by warp shuffles -- then writes
+//   U[:, c]  = T * M[J, c]     (c not in J),   U[:, J] = T        (kSw x Cc)
+//   Pc[i, :] = M[i, J]         (i not in J),   Pc[J, :] = -I      (R x kSw)
+// for its chunk of columns / rows.  T = M[J,J]^{-1}.
+// ---------------------------------------------------------------------------
+constexpr int kSw = 32;  // pivot-block width (K of the rank-kSw update)
+
+__device__ void invert_block(double2 (*Ts)[kSw + 1], int* perm, int jn, int* status) {
+  __shared__ int piv_s;
+  __shared__ double2 prow[kSw], fcol[kSw];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  for (int p = 0; p < jn; p++) {
+    if (warp == 0) {
+      double mag = (lane >= p && lane < jn) ? cabs2(Ts[lane][p]) : -1.0;
+      int idx = lane;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        double om = __shfl_down_sync(0xffffffffu, mag, off);
+        int oi = __shfl_down_sync(0xffffffffu, idx, off);
+        if (om > mag || (om == mag && oi < idx)) { mag = om; idx = oi; }
+      }
+      if (lane == 0) {
+        piv_s = idx;
+        if (!(mag > 0.0) || !isfinite(mag)) atomicOr(status, kStatusSingular);
+      }
+    }
+    __syncthreads();
+    const int q = piv_s;
+    if (q != p && t < kSw) {
+      double2 tmp = Ts[p][t];
+      Ts[p][t] = Ts[q][t];
+      Ts[q][t] = tmp;
+      if (t == 0) { int ti = perm[p]; perm[p] = perm[q]; perm[q] = ti; }
+    }
+    __syncthreads();
+    const double2 d = cinv(Ts[p][p]);
+    if (t < kSw) {
+      prow[t] = (t == p) ? d : cmul(Ts[p][t], d);
+      fcol[t] = Ts[t][p];
+    }
+    __syncthreads();
+    for (int e = t; e < kSw * kSw; e += blockDim.x) {
+      int i = e / kSw, j = e % kSw;
+      if (i == p) Ts[i][j] = prow[j];
+      else if (j == p) Ts[i][j] = cneg(cmul(fcol[i], d));
+      else Ts[i][j] = csub(Ts[i][j], cmul(fcol[i], prow[j]));
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) k_sweep_panel(const double2* __restrict__ M, int64_t ldm, int64_t R,
+                                                     int64_t Cc, int64_t j0, int jn, double2* __restrict__ Pc,
+                                                     double2* __restrict__ U, int64_t ldu, int* status) {
+  __shared__ double2 Ts[kSw][kSw + 1];
+  __shared__ double2 Ms[kSw][kSw + 1];
+  __shared__ int perm[kSw], pinv[kSw];
+  const int t = threadIdx.x;
+  for (int e = t; e < kSw * kSw; e += blockDim.x) {
+    int i = e / kSw, j = e % kSw;
+    Ts[i][j] = (i < jn && j < jn) ? M[(j0 + i) * ldm + j0 + j] : cmk(i == j ? 1.0 : 0.0, 0.0);
+  }
+  if (t < kSw) perm[t] = t;
+  __syncthreads();
+  invert_block(Ts, perm, jn, status);
+  // the pivoted sweep leaves inv(P M_JJ) = inv(M_JJ) P^T: inv(M_JJ)[r][c] = Ts[r][pinv[c]]
+  if (t < kSw) pinv[perm[t]] = t;
+  __syncthreads();
+  // U for columns [c0, c0+64), in two 32-wide chunks
+  const int64_t c0 = (int64_t)blockIdx.x * 64;
+  for (int sub = 0; sub < 2; sub++) {
+    const int64_t cb = c0 + sub * kSw;
+    if (cb >= Cc) break;
+    for (int e = t; e < kSw * kSw; e += blockDim.x) {
+      int q = e / kSw, c = e % kSw;
+      int64_t gc = cb + c;
+      Ms[q][c] = (q < jn && gc < Cc) ? M[(j0 + q) * ldm + gc] : cmk(0.0, 0.0);
+    }
+    __syncthreads();
+    for (int e = t; e < kSw * kSw; e += blockDim.x) {
+      int r = e / kSw, c = e % kSw;
+      int64_t gc = cb + c;
+      if (gc >= Cc) continue;
+      double2 v = cmk(0.0, 0.0);
+      if (r < jn) {
+        if (gc >= j0 && gc < j0 + jn) {
+          v = Ts[r][pinv[gc - j0]];
+        } else {
+          for (int q = 0; q < jn; q++) v = cadd(v, cmul(Ts[r][pinv[q]], Ms[q][c]));
+        }
+      }
+      U[r * ldu + gc] = v;
+    }
+    __syncthreads();
+  }
+  // Pc for rows [r0, r0+64)
+  const int64_t r0 = (int64_t)blockIdx.x * 64;
+  if (r0 < R) {
+    for (int e = t; e < 64 * kSw; e += blockDim.x) {
+      int r = e / kSw, q = e % kSw;
+      int64_t gr = r0 + r;
+      if (gr >= R) continue;
+      double2 v;
+      if (gr >= j0 && gr < j0 + jn) v = cmk((gr - j0 == q) ? -1.0 : 0.0, 0.0);
+      else v = (q < jn) ? M[gr * ldm + j0 + q] : cmk(0.0, 0.0);
+      Pc[gr * kSw + q] = v;
+    }
+  }
+}
+
+void launch_sweep_panel(const double2* M, int64_t ldm, int64_t R, int64_t Cc, int64_t j0, int jn, double2* Pc,
+                        double2* U, int64_t ldu, int* status, cudaStream_t s) {
+  int64_t nblk = ((R > Cc ? R : Cc) + 63) / 64;
+  k_sweep_panel<<<(unsigned)nblk, 256, 0, s>>>(M, ldm, R, Cc, j0, jn, Pc, U, ldu, status);
+}
+
+void launch_sweep_update(double2* M, int64_t ldm, int64_t R, int64_t Cc, int64_t j0, int jn, const double2* Pc,
+                         const double2* U, int64_t ldu, cudaStream_t s) {
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_zgemm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
+    attr = true;
+  }
+  ZOp A{Pc, kSw, 0}, B{U, ldu, 0};
+  dim3 grid((unsigned)((Cc + kBN - 1) / kBN), (unsigned)((R + kBM - 1) / kBM));
+  k_zgemm<true><<<grid, 128, kGemmSmem, s>>>(R, Cc, kSw, cmk(-1.0, 0.0), A, B, cmk(1.0, 0.0), M, ldm, j0, jn);
+}
+
+const char* sweep_update_kernel_name() { return "k_zgemm<true> (sweep rank-32 update, FP64 DMMA)"; }
+
+int sweep_block_width() { return kSw; }
+
+// ---------------------------------------------------------------------------
+// Slice assembly: rows [0, N) x cols [0, N) of the augmented matrix become
+//   A0 - k0dx^2 diag(eps) - G_src (- G_extra)
+// (cal_smatrix_RGF.m:264-265; the attach step uses G_extra = G0 of the far
+// lead, since (I - G0 G)^{-1} G0 = (G0^{-1} - G)^{-1} with G0^{-1} = A_lead - G0).
+// Rows [N, Rz) x cols [0, N) are negated (-Z).  eps == nullptr means the
+// uniform permittivity eps_u.
+// ---------------------------------------------------------------------------
+__global__ void k_assemble(double2* M, int64_t ldm, int64_t N, int64_t Rz, const double2* Gsrc,
+                           int64_t ldg, const double2* Gextra, int64_t lde, const int* st_col,
+                           const double2* st_val, double2 k2, const double2* eps, double2 eps_u) {
+  int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int64_t i = blockIdx.y;
+  for (; i < Rz; i += gridDim.y) {
+    if (j >= N) return;
+    if (i >= N) {
+      M[i * ldm + j] = cneg(M[i * ldm + j]);
+      continue;
+    }
+    double2 v = cneg(Gsrc[i * ldg + j]);
+    if (Gextra) v = csub(v, Gextra[i * lde + j]);
+#pragma unroll
+    for (int q = 0; q < kMaxStencil; q++)
+      if (st_col[i * kMaxStencil + q] == j) v = cadd(v, st_val[i * kMaxStencil + q]);
+    if (i == j) v = csub(v, cmul(k2, eps ? eps[i] : eps_u));
+    M[i * ldm + j] = v;
+  }
+}
+
+void launch_assemble(double2* M, int64_t ldm, int64_t N, int64_t Rz, const double2* Gsrc, int64_t ldg,
+                     const double2* Gextra, int64_t lde, const int* st_col, const double2* st_val,
+                     double2 k2, const double2* eps, double2 eps_u, cudaStream_t s) {
+  dim3 grid((unsigned)((N + 127) / 128), (unsigned)(Rz < 8192 ? Rz : 8192));
+  k_assemble<<<grid, 128, 0, s>>>(M, ldm, N, Rz, Gsrc, ldg, Gextra, lde, st_col, st_val, k2, eps, eps_u);
+}
+
+// ---------------------------------------------------------------------------
+// Carrier blocks.  With p = prop index of a requested channel, lam = exp(i kx)
+// and mu = sqrt_mu (cal_smatrix_RGF.m:191-203):
+//   init  : X0 = G0_s B_s = phi(:,p) lam_p mu_p,   -Z0 = -(C_s G0_s) = -mu_p lam_p phi(:,p)^H,
+//           Y0 = C_s G0_s B_s = mu lam mu on coinciding channels   (phi is unitary)
+//   attach: B_e = phi(:,p) mu_p (extra columns),   -C_e = -mu_p phi(:,p)^H (extra rows)
+// ---------------------------------------------------------------------------
+__global__ void k_fill_init(double2* M, int64_t ldm, int64_t N, const double2* phi, int64_t ldp,
+                            const int* prop, const double2* lam, const double2* mu, const int* in_s,
+                            int n_in, const int* out_s, int n_out) {
+  int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int64_t nx = N * n_in, nz = (int64_t)n_out * N, ny = (int64_t)n_out * n_in;
+  if (idx < nx) {
+    int64_t m = idx / n_in;
+    int i = (int)(idx % n_in);
+    int p = prop[in_s[i]];
+    M[m * ldm + N + i] = cmul(phi[m * ldp + p], cmul(lam[p], mu[p]));
+  } else if (idx < nx + nz) {
+    int64_t e = idx - nx;
+    int o = (int)(e / N);
+    int64_t m = e % N;
+    int p = prop[out_s[o]];
+    M[(N + o) * ldm + m] = cneg(cmul(cmul(mu[p], lam[p]), cconj(phi[m * ldp + p])));
+  } else if (idx < nx + nz + ny) {
+    int64_t e = idx - nx - nz;
+    int o = (int)(e / n_in), i = (int)(e % n_in);
+    int po = prop[out_s[o]], pi = prop[in_s[i]];
+    M[(N + o) * ldm + N + i] = (po == pi) ? cmul(cmul(mu[po], lam[po]), mu[pi]) : cmk(0.0, 0.0);
+  }
+}
+
+void launch_fill_init(double2* M, int64_t ldm, int64_t N, const double2* phi, int64_t ldp, const int* prop,
+                      const double2* lam, const double2* mu, const int* in_s, int n_in, const int* out_s,
+                      int n_out, cudaStream_t s) {
+  int64_t tot = N * n_in + (int64_t)n_out * N + (int64_t)n_out * n_in;
+  if (tot == 0) return;
+  k_fill_init<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(M, ldm, N, phi, ldp, prop, lam, mu, in_s, n_in,
+                                                            out_s, n_out);
+}
+
+// attach-step extra rows/columns; rows [N, N+no_s) and columns [N, N+ni_s)
+// hold the carried Z/X, the new ones follow them.
+__global__ void k_fill_attach(double2* M, int64_t ldm, int64_t N, int ni_s, int no_s, const double2* phi,
+                              int64_t ldp, const int* prop, const double2* mu, const int* in_e, int ni_e,
+                              const int* out_e, int no_e) {
+  int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t Ct = N + ni_s + ni_e;
+  int64_t nb = N * ni_e;                        // B_e block
+  int64_t nzr = (int64_t)no_s * ni_e;           // zeros: Z rows x B_e cols
+  int64_t nc = (int64_t)no_e * Ct;              // whole C_e rows
+  if (idx < nb) {
+    int64_t m = idx / ni_e;
+    int i = (int)(idx % ni_e);
+    int p = prop[in_e[i]];
+    M[m * ldm + N + ni_s + i] = cmul(phi[m * ldp + p], mu[p]);
+  } else if (idx < nb + nzr) {
+    int64_t e = idx - nb;
+    int64_t o = e / ni_e, i = e % ni_e;
+    M[(N + o) * ldm + N + ni_s + i] = cmk(0.0, 0.0);
+  } else if (idx < nb + nzr + nc) {
+    int64_t e = idx - nb - nzr;
+    int o = (int)(e / Ct);
+    int64_t c = e % Ct;
+    double2 v = cmk(0.0, 0.0);
+    if (c < N) {
+      int p = prop[out_e[o]];
+      v = cneg(cmul(mu[p], cconj(phi[c * ldp + p])));
+    }
+    M[(N + no_s + o) * ldm + c] = v;
+  }
+}
+
+void launch_fill_attach(double2* M, int64_t ldm, int64_t N, int ni_s, int no_s, const double2* phi,
+                        int64_t ldp, const int* prop, const double2* mu, const int* in_e, int ni_e,
+                        const int* out_e, int no_e, cudaStream_t s) {
+  int64_t tot = N * ni_e + (int64_t)no_s * ni_e + (int64_t)no_e * (N + ni_s + ni_e);
+  if (tot == 0) return;
+  k_fill_attach<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(M, ldm, N, ni_s, no_s, phi, ldp, prop, mu,
+                                                              in_e, ni_e, out_e, no_e);
+}
+
+// ---------------------------------------------------------------------------
+// Fisher-Lee extraction (cal_smatrix_RGF.m:279, 286-289):
+//   S(o, i) = -2i * W[N + row_of[o], N + col_of[i]] - delta(o, i)
+// written column-major with leading dimension ldS; delta pairs come from the
+// host (MATLAB intersect semantics).
+// ---------------------------------------------------------------------------
+__global__ void k_extract(const double2* M, int64_t ldm, int64_t N, const int* row_of, int no,
+                          const int* col_of, int ni, double2* S, int64_t ldS) {
+  int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)no * ni) return;
+  int o = (int)(idx % no), i = (int)(idx / no);
+  double2 w = M[(N + row_of[o]) * ldm + N + col_of[i]];
+  S[o + (int64_t)i * ldS] = cmk(2.0 * w.y, -2.0 * w.x);
+}
+
+__global__ void k_delta(double2* S, int64_t ldS, const int* pairs, int npairs) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= npairs) return;
+  int o = pairs[2 * k], i = pairs[2 * k + 1];
+  S[o + (int64_t)i * ldS].x -= 1.0;
+}
+
+void launch_extract(const double2* M, int64_t ldm, int64_t N, const int* row_of, int no, const int* col_of,
+                    int ni, double2* S, int64_t ldS, const int* pairs, int npairs, cudaStream_t s) {
+  int64_t tot = (int64_t)no * ni;
+  if (tot > 0) k_extract<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(M, ldm, N, row_of, no, col_of, ni, S, ldS);
+  if (npairs > 0) k_delta<<<(npairs + 255) / 256, 256, 0, s>>>(S, ldS, pairs, npairs);
+}
+
+// ---------------------------------------------------------------------------
+// misc
+// ---------------------------------------------------------------------------
+__global__ void k_check_finite(const double2* x, int64_t n, int* status) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  bool bad = false;
+  for (; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double2 v = x[i];
+    if (!isfinite(v.x) || !isfinite(v.y)) bad = true;
+  }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(status, kStatusNonfinite);
+}
+
+void launch_check_finite(const double2* x, int64_t n, int* status, cudaStream_t s) {
+  if (n <= 0) return;
+  int64_t blocks = (n + 255) / 256;
+  if (blocks > 1184) blocks = 1184;
+  k_check_finite<<<(unsigned)blocks, 256, 0, s>>>(x, n, status);
+}
+
+// dst[r*ldd + c] = src[r*lds + c] * diag[c]  (phi * diag(exp(1i*kx)) for G0)
+__global__ void k_scale_cols(const double2* src, int64_t lds, const double2* diag, double2* dst, int64_t ldd,
+                             int64_t rows, int64_t cols) {
+  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  for (int64_t r = blockIdx.y; r < rows; r += gridDim.y)
+    if (c < cols) dst[r * ldd + c] = cmul(src[r * lds + c], diag[c]);
+}
+
+void launch_scale_cols(const double2* src, int64_t lds, const double2* diag, double2* dst, int64_t ldd,
+                       int64_t rows, int64_t cols, cudaStream_t s) {
+  dim3 grid((unsigned)((cols + 127) / 128), (unsigned)(rows < 8192 ? rows : 8192));
+  k_scale_cols<<<grid, 128, 0, s>>>(src, lds, diag, dst, ldd, rows, cols);
+}
+
+}  // namespace rgf

@@ -1,0 +1,38 @@
+// Slice-recursion kernels (see sweep.cu).
+#pragma once
+#include "rgf_internal.cuh"
+
+namespace rgf {
+
+// operand of the complex GEMM: element (r, c) of the logical matrix is
+// p[r*ld + c] (op 0), p[c*ld + r] (op 1) or conj(p[c*ld + r]) (op 2)
+struct ZOp {
+  const double2* p;
+  int64_t ld;
+  int op;
+};
+
+void launch_zgemm(int64_t M, int64_t N, int64_t K, double2 alpha, ZOp A, ZOp B, double2 beta, double2* C,
+                  int64_t ldc, cudaStream_t s);
+int sweep_block_width();
+void launch_sweep_panel(const double2* M, int64_t ldm, int64_t R, int64_t Cc, int64_t j0, int jn, double2* Pc,
+                        double2* U, int64_t ldu, int* status, cudaStream_t s);
+void launch_sweep_update(double2* M, int64_t ldm, int64_t R, int64_t Cc, int64_t j0, int jn, const double2* Pc,
+                         const double2* U, int64_t ldu, cudaStream_t s);
+const char* sweep_update_kernel_name();
+void launch_assemble(double2* M, int64_t ldm, int64_t N, int64_t Rz, const double2* Gsrc, int64_t ldg,
+                     const double2* Gextra, int64_t lde, const int* st_col, const double2* st_val, double2 k2,
+                     const double2* eps, double2 eps_u, cudaStream_t s);
+void launch_fill_init(double2* M, int64_t ldm, int64_t N, const double2* phi, int64_t ldp, const int* prop,
+                      const double2* lam, const double2* mu, const int* in_s, int n_in, const int* out_s,
+                      int n_out, cudaStream_t s);
+void launch_fill_attach(double2* M, int64_t ldm, int64_t N, int ni_s, int no_s, const double2* phi,
+                        int64_t ldp, const int* prop, const double2* mu, const int* in_e, int ni_e,
+                        const int* out_e, int no_e, cudaStream_t s);
+void launch_extract(const double2* M, int64_t ldm, int64_t N, const int* row_of, int no, const int* col_of,
+                    int ni, double2* S, int64_t ldS, const int* pairs, int npairs, cudaStream_t s);
+void launch_check_finite(const double2* x, int64_t n, int* status, cudaStream_t s);
+void launch_scale_cols(const double2* src, int64_t lds, const double2* diag, double2* dst, int64_t ldd,
+                       int64_t rows, int64_t cols, cudaStream_t s);
+
+}  // namespace rgf
