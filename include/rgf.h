@@ -111,7 +111,8 @@ typedef struct {
 
 typedef struct {
   int32_t precision;  /* rgf_precision (0 = RGF_FP64)                                  */
-  int32_t block;      /* reserved: pivot-block width of the slice inverse (0 = default)*/
+  int32_t engine;     /* 0: persistent register-resident sweep kernel when the matrix
+                         fits on the GPU (default), 1: one launch pair per pivot step */
   int32_t S_on_device;/* 1: S is a device pointer (no D2H copy)                        */
   int32_t profile;    /* > 0: time the dominant kernel with CUDA events on every
                          profile-th slice (read back with rgf_last_profile)           */

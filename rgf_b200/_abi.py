@@ -52,7 +52,7 @@ class Request(ctypes.Structure):
 
 
 class Options(ctypes.Structure):
-    _fields_ = [("precision", c_int32), ("block", c_int32), ("S_on_device", c_int32), ("profile", c_int32)]
+    _fields_ = [("precision", c_int32), ("engine", c_int32), ("S_on_device", c_int32), ("profile", c_int32)]
 
 
 class Channels(ctypes.Structure):

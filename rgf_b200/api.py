@@ -219,7 +219,7 @@ def _options(options) -> Options:
         return Options(_abi.RGF_FP64, 0, 0, 0)
     if isinstance(options, Options):
         return options
-    return Options(int(options.get("precision", 0)), int(options.get("block", 0)),
+    return Options(int(options.get("precision", 0)), int(options.get("engine", 0)),
                    int(options.get("S_on_device", 0)), 0)
 
 

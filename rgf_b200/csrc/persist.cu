@@ -1,0 +1,1010 @@
+// Persistent slice-recursion kernel (FP64 plain form).
+//
+// One cooperative launch runs the L slice sweeps of cal_smatrix_RGF.m:263-269
+// (any of the five branches, projected on the requested channels; sweep.cu
+// explains the augmented-matrix formulation).  The active augmented matrix W
+// (R x C) is cut into TR x TC tiles of BM x BN; CTA (I, Cq) keeps its tile in
+// FP64 DMMA accumulator registers for the whole recursion, so W goes back to
+// memory only once per slice (for the slice assembly).
+//
+// Pivot step s (block J_s = [j0, j0+jn), jn <= 32) of the Gauss-Jordan sweep:
+//     W <- W_mod + Pc * U,  Pc = [-W(i,J) (i not in J) ; +I (i in J)]
+//                           U  = T_s * [W(J,c) (c not in J) | I (c in J)],  T_s = W(J,J)^{-1}
+// where W_mod is W with the rows and columns of J zeroed.  Roles:
+//  * tile CTA, 2 math warpgroups: wait for Pc(I) and U(Cq) of step s, stage
+//    them in shared memory with TMA bulk copies (cp.async.bulk + mbarrier) and
+//    update the register tile with mma.sync.m8n8k4.f64.  The subtiles holding
+//    pieces of later steps go first and are published right away: the pivot
+//    rows W(J_{s+1}, Cq) and columns W(I, J_{s+1}) of step s+1, and three
+//    32x32 blocks of W after step s -- (J_{s+2},J_{s+2}), (J_{s+2},J_{s+1}),
+//    (J_{s+1},J_{s+2}) -- for the T-server.
+//  * tile CTA, 1 panel warpgroup: its ceil(BN/TR)-column slice of U_s(Cq),
+//    on the FP64 tensor cores.
+//  * T-server CTA (one extra CTA on an SM of its own, so its FP64 pipe is not
+//    shared with the bulk update): one step ahead of the bulk it forms the
+//    next pivot block as the Schur update
+//        W^{(s-1)}(J_s,J_s) = W^{(s-2)}(J_s,J_s) - W^{(s-2)}(J_s,J_{s-1}) T_{s-1} W^{(s-2)}(J_{s-1},J_s)
+//    (W^{(s)} = W after step s) and inverts it by register-resident
+//    Gauss-Jordan with partial pivoting (redux.sync pivot search, implicit row
+//    interchanges, one barrier per pivot); the first pivot block of every
+//    slice comes straight from the slice assembly.
+// setmaxnreg moves registers from the panel warpgroup (88) to the math
+// warpgroups (208) so the 96x96 complex tile (144 registers/thread) fits.
+// Exchange buffers are double-buffered by step parity; each has a publication
+// flag (release/acquire, holds the step number) and a consumption counter the
+// next writer of that parity waits on.  Every wait is bounded by a clock
+// budget; on expiry the kernel sets kStatusTimeout, raises a global abort word
+// that all other waits poll, and every role returns uniformly.
+//
+// A probe pair of columns (p1 = v, p2 = M_n v) rides along: after slice n, p2
+// holds G_n M_n v, and max |G_n M_n v - v| bounds the error of every slice
+// inverse a posteriori.
+#include <math.h>
+
+#include "persist.cuh"
+
+namespace rgf {
+
+namespace {
+
+constexpr int kPB = 32;  // pivot block width
+constexpr int kPanelWarps = 4, kPanelThreads = kPanelWarps * 32;  // one warpgroup
+constexpr int kBarMath = 1, kBarPanel = 2, kBarPub = 3, kBarDjj = 4, kBarSrv = 5;  // named barriers
+constexpr int kMaxTile = 96;
+constexpr int kServerThreads = 256;  // the math warpgroups of the T-server CTA
+constexpr unsigned kFull = 0xffffffffu;
+
+template <int BM, int BN>
+struct Cfg {
+  static constexpr int WM = 2, WN = 4;  // math warp grid
+  static constexpr int MathWarps = WM * WN, MathThreads = MathWarps * 32;
+  static constexpr int Threads = MathThreads + kPanelThreads;
+  static constexpr int MathRegs = 208, PanelRegs = 88;  // 256*208 + 128*88 = 384*168
+};
+
+// Named barriers in their non-.aligned form (per-thread arrival), preceded
+// by a warp reconvergence, so that no barrier depends on the compiler having
+// reconverged a warp after lane-divergent code.
+__device__ __forceinline__ void bar_sync(int id, int n) {
+  __syncwarp();
+  asm volatile("barrier.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+// CTA-uniform OR over the threads of a named barrier
+__device__ __forceinline__ int bar_or(int id, int n, int pred) {
+  int r;
+  __syncwarp();
+  asm volatile(
+      "{ .reg .pred p, q; setp.ne.s32 p, %3, 0; barrier.red.or.pred q, %1, %2, p; selp.s32 %0, 1, 0, q; }"
+      : "=r"(r)
+      : "r"(id), "r"(n), "r"(pred)
+      : "memory");
+  return r;
+}
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+// volatile keeps predicated products from being if-converted into
+// unconditional ones; callers order the issue so that the two dependent
+// DMMAs of each complex product are far apart
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// 1/z = conj(z) / |z|^2 with the real reciprocal 1/n refined by two
+// Newton-Raphson steps r <- r + r (1 - n r) from a single-precision seed
+// (quadratic convergence: ~24 -> ~48 -> full double precision); IEEE
+// division outside the single-precision range
+__device__ __forceinline__ double2 crecip(double2 z) {
+  const double n = z.x * z.x + z.y * z.y;
+  double r;
+  if (n > 1e-30 && n < 1e30) {
+    r = (double)(1.0f / (float)n);
+    double e = fma(-n, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-n, r, 1.0);
+    r = fma(r, e, r);
+  } else {
+    r = 1.0 / n;
+  }
+  return cmk(z.x * r, -z.y * r);
+}
+
+// swizzled element positions of the staged operand tiles (conflict-free
+// m8n8k4 fragment loads): A is [BM][32], B is [32][BN]
+__device__ __forceinline__ int swzA(int r, int k) { return r * kPB + (k ^ ((r & 1) << 2)); }
+template <int BN>
+__device__ __forceinline__ int swzB(int k, int c) { return k * BN + (c ^ ((k & 3) << 1)); }
+
+typedef double2 Blk[kPB][kPB + 1];  // padded 32x32 block in shared memory
+
+struct Shared {
+  union {
+    struct {  // tile CTAs, math role: staged operands of the current step
+      alignas(128) double2 A[kMaxTile * kPB];
+      alignas(128) double2 B[kPB * kMaxTile];
+    } op;
+    struct {  // T-server CTA: the three published blocks, T_{s-1}, scratch
+      Blk a1, a2, a3, tprev, v;
+    } srv;
+  };
+  alignas(8) unsigned long long mbar;
+  int math_abort;
+  int panel_abort;
+  Blk T;   // panel role: T_s
+  Blk Mr;  // panel role: my columns of the pivot rows
+  double2 fcol[2][kPB];
+  double2 dpiv[2];
+  int piv[2];
+  int perm[kPB], pinv[kPB];
+};
+
+__device__ __forceinline__ void trace_ev(const PersistParams& p, int s, int ev) {
+  if (p.trace && s >= 0 && s < p.trace_steps)
+    p.trace[((size_t)blockIdx.x * p.trace_steps + s) * kTraceEvents + ev] = gtimer();
+}
+
+__device__ __forceinline__ bool give_up(const PersistParams& p, long long t0) {
+  if (*(volatile const int*)p.abort) return true;
+  if (clock64() - t0 > p.timeout_cycles) {
+    atomicOr(p.status, kStatusTimeout);
+    atomicExch(p.abort, 1);
+    return true;
+  }
+  return false;
+}
+
+// bounded wait on a flag word; false = gave up (timeout here or abort raised elsewhere)
+__device__ bool wait_ge(const PersistParams& p, const int* flag, int target) {
+  if (ld_acquire(flag) >= target) return true;
+  const long long t0 = clock64();
+  for (int spins = 1;; spins++) {
+    if (spins > 64) __nanosleep(32);
+    if (ld_acquire(flag) >= target) return true;
+    if ((spins & 63) == 0 && give_up(p, t0)) return false;
+  }
+}
+
+// one warp waits until flags[0..count) >= target and, if extra != nullptr,
+// *extra >= target; the flags are polled in parallel, one per lane.  Returns
+// the same verdict in every lane.
+__device__ bool warp_wait_all(const PersistParams& p, const int* flags, int count, const int* extra, int target) {
+  const int lane = threadIdx.x & 31;
+  const long long t0 = clock64();
+  for (int spins = 0;; spins++) {
+    bool mine = true;
+    for (int r = lane; r < count; r += 32) mine = mine && (ld_acquire(flags + r) >= target);
+    if (lane == 0 && extra) mine = mine && (ld_acquire(extra) >= target);
+    if (__all_sync(kFull, mine)) return true;
+    if (spins > 64) __nanosleep(32);
+    if ((spins & 63) == 63) {
+      const int bad = (lane == 0) ? (int)give_up(p, t0) : 0;
+      if (__shfl_sync(kFull, bad, 0)) return false;
+    }
+  }
+}
+
+// Flag words.  A flag of a buffer with several writers (the server blocks)
+// is kept per step parity: the same-parity value can only advance after the
+// server consumed the previous one, so "flag >= s" means "published for s".
+struct Sync {
+  int *pc_flag, *row_flag, *t_flag, *u_flag, *d_flag, *srv_flag, *d_used;
+  int *pc_cons, *row_cons, *t_cons, *u_cons, *srv_cons;
+  __device__ explicit Sync(const PersistParams& p) {
+    pc_flag = p.flags;
+    row_flag = pc_flag + p.TR;
+    t_flag = row_flag + p.TC;
+    u_flag = t_flag + 1;
+    d_flag = u_flag + p.TR * p.TC;
+    srv_flag = d_flag + 1;
+    d_used = srv_flag + 6;
+    pc_cons = p.cons;
+    row_cons = pc_cons + 2 * p.TR;
+    t_cons = row_cons + 2 * p.TC;
+    u_cons = t_cons + 2;
+    srv_cons = u_cons + 2 * p.TC;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// tile CTA, math warpgroups
+// ---------------------------------------------------------------------------
+template <int BM, int BN>
+struct MathTile {
+  static constexpr int WR = BM / Cfg<BM, BN>::WM, WC = BN / Cfg<BM, BN>::WN;  // warp tile
+  static constexpr int MI = WR / 8, NI = WC / 8;
+  double acc[MI][NI][4];  // {re(c), re(c+1), im(c), im(c+1)}
+  int lane, wr, wc;
+  int r_base, c_base;
+  __device__ int row(int mi) const { return r_base + mi * 8 + (lane >> 2); }
+  __device__ int col(int ni, int h) const { return c_base + ni * 8 + (lane & 3) * 2 + h; }
+};
+
+__device__ __forceinline__ double2 assemble_elem(const PersistParams& p, int64_t i, int64_t j, double2 v,
+                                                 const double2* eps_next) {
+  if (j < p.N) {
+    if (i < p.N) {
+      double2 a = cneg(v);
+#pragma unroll
+      for (int q = 0; q < kMaxStencil; q++)
+        if (p.st_col[i * kMaxStencil + q] == j) a = cadd(a, p.st_val[i * kMaxStencil + q]);
+      if (i == j) a = csub(a, cmul(p.k2, eps_next[i]));
+      return a;
+    }
+    return cneg(v);  // -Z rows
+  }
+  return v;  // X columns and the Y block are carried unchanged
+}
+
+// Slice boundary on this CTA's tile of W (global memory): probe check
+// (p2 = G_n M_n v against v) and, when eps_next is given, the assembly of the
+// next slice matrix: top-left A_{n+1} - G_n, -Z rows, probe pair
+// p1 = v, p2 = A_{n+1} v - G_n v.  Returns the largest probe residual seen.
+template <int BM, int BN>
+__device__ double boundary_pass(const PersistParams& p, int I, int Cq, int tid, int nthreads,
+                                const double2* eps_next) {
+  double pmax = 0.0;
+  const int64_t r0 = (int64_t)I * BM, c0 = (int64_t)Cq * BN;
+  const int pc1 = p.pc1;
+  for (int e = tid; e < BM * BN; e += nthreads) {
+    const int64_t i = r0 + e / BN, j = c0 + e % BN;
+    if (i >= p.R || j >= p.C) continue;
+    double2* w = p.M + i * p.ldm + j;
+    if (pc1 >= 0 && (j == pc1 || j == pc1 + 1)) {
+      if (j != pc1) continue;  // the thread of column p1 handles the pair
+      double2* w2 = w + 1;
+      if (i < p.N) {
+        const double2 v = probe_v(i);
+        const double2 d = csub(__ldcg(w2), v);
+        pmax = fmax(pmax, sqrt(cabs2(d)));
+        if (eps_next) {
+          double2 Av = cmk(0.0, 0.0);
+          for (int q = 0; q < kMaxStencil; q++) {
+            const int cq = p.st_col[i * kMaxStencil + q];
+            if (cq >= 0) Av = cadd(Av, cmul(p.st_val[i * kMaxStencil + q], probe_v(cq)));
+          }
+          Av = csub(Av, cmul(cmul(p.k2, eps_next[i]), v));
+          const double2 Gv = __ldcg(w);
+          __stcg(w, v);
+          __stcg(w2, csub(Av, Gv));
+        }
+      } else if (eps_next) {
+        __stcg(w, cmk(0.0, 0.0));
+        __stcg(w2, cmk(0.0, 0.0));
+      }
+      continue;
+    }
+    if (eps_next) __stcg(w, assemble_elem(p, i, j, __ldcg(w), eps_next));
+  }
+  return pmax;
+}
+
+template <int BM, int BN>
+__device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, int I, int Cq) {
+  using Tile = MathTile<BM, BN>;
+  constexpr int MI = Tile::MI, NI = Tile::NI;
+  constexpr int kMathWarps = Cfg<BM, BN>::MathWarps, kMathThreads = Cfg<BM, BN>::MathThreads;
+  Tile t;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  t.lane = tid & 31;
+  t.wr = warp >> 2;
+  t.wc = warp & 3;
+  t.r_base = I * BM + t.wr * Tile::WR;
+  t.c_base = Cq * BN + t.wc * Tile::WC;
+  const int S = p.L * p.NB;
+  const int tr0 = I * BM, tc0 = Cq * BN;  // tile origin
+
+  // Urgent subtiles of this warp for the pieces published while step s runs:
+  // rows / columns of the window of step s1 = s+1 (rowU/colU) and, when s2 =
+  // s1+1 is in the same slice, the block (J_s2, J_s2) (rowU2 && colU2); the
+  // server blocks (J_s2,J_s1) and (J_s1,J_s2) lie inside colU / rowU.
+  // (bit mi / ni of the masks below)
+  unsigned rowU = 0, colU = 0, rowU2 = 0, colU2 = 0;
+  bool any_r = false, any_c = false, any_srv = false, any_urg = false;
+  auto set_urgency = [&](int s1, bool with_srv) {
+    const int w1 = (s1 % p.NB) * kPB, w2 = w1 + kPB;
+    rowU = colU = rowU2 = colU2 = 0;
+#pragma unroll
+    for (int mi = 0; mi < MI; mi++) {
+      const int r0 = t.r_base + mi * 8;
+      rowU |= (unsigned)(r0 >= w1 && r0 < w1 + kPB) << mi;
+      rowU2 |= (unsigned)(with_srv && r0 >= w2 && r0 < w2 + kPB) << mi;
+    }
+#pragma unroll
+    for (int ni = 0; ni < NI; ni++) {
+      const int c0 = t.c_base + ni * 8;
+      colU |= (unsigned)(c0 >= w1 && c0 < w1 + kPB) << ni;
+      colU2 |= (unsigned)(with_srv && c0 >= w2 && c0 < w2 + kPB) << ni;
+    }
+    any_r = rowU != 0;
+    any_c = colU != 0;
+    any_srv = (rowU2 && colU2) || (rowU2 && colU) || (rowU && colU2);
+    any_urg = any_r || any_c || (rowU2 && colU2);
+  };
+  auto clear_urgency = [&]() {
+    any_r = any_c = any_srv = any_urg = false;
+    rowU = colU = rowU2 = colU2 = 0;
+  };
+  auto bit = [](unsigned m, int i) { return ((m >> i) & 1u) != 0; };
+  // The warps of this CTA that publish a kind of piece for step s1, and the
+  // lowest of them (the one that releases the flags), computed on demand so
+  // that nothing of it stays live across the update passes.
+  enum { kSetGlob, kSetDjj, kSetSrv };
+  auto pub_set = [&](int kind, int s1, int* lead) {
+    const int w1 = (s1 % p.NB) * kPB, w2 = w1 + kPB;
+    int n = 0;
+    *lead = -1;
+    for (int w = kMathWarps - 1; w >= 0; w--) {
+      const int rb = tr0 + (w >> 2) * Tile::WR, cb = tc0 + (w & 3) * Tile::WC;
+      const bool r1 = (w1 + kPB > rb) && (w1 < rb + Tile::WR);
+      const bool c1 = (w1 + kPB > cb) && (w1 < cb + Tile::WC);
+      const bool r2 = (w2 + kPB > rb) && (w2 < rb + Tile::WR);
+      const bool c2 = (w2 + kPB > cb) && (w2 < cb + Tile::WC);
+      const bool in = kind == kSetGlob ? (r1 || c1) : kind == kSetDjj ? (r1 && c1) : ((r2 && c2) || (r2 && c1) || (r1 && c2));
+      if (in) {
+        n++;
+        *lead = w;
+      }
+    }
+    return n;
+  };
+  auto load_tile = [&]() {
+#pragma unroll
+    for (int mi = 0; mi < MI; mi++)
+#pragma unroll
+      for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int i = t.row(mi), j = t.col(ni, h);
+          const double2 v = (i < p.R && j < p.C) ? __ldcg(p.M + (int64_t)i * p.ldm + j) : cmk(0.0, 0.0);
+          t.acc[mi][ni][h] = v.x;
+          t.acc[mi][ni][2 + h] = v.y;
+        }
+  };
+  auto store_tile = [&]() {
+#pragma unroll
+    for (int mi = 0; mi < MI; mi++)
+#pragma unroll
+      for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int i = t.row(mi), j = t.col(ni, h);
+          if (i < p.R && j < p.C) __stcg(p.M + (int64_t)i * p.ldm + j, cmk(t.acc[mi][ni][h], t.acc[mi][ni][2 + h]));
+        }
+  };
+  // rank-32 update of a subset of this warp's subtiles: 0 all, 1 urgent, 2 the rest.
+  // First halves of every complex product, then the dependent second halves.
+  auto mma_pass = [&](const int mode) {
+    auto sel = [&](int mi, int ni) {
+      const bool u = bit(rowU, mi) || bit(colU, ni) || (bit(rowU2, mi) && bit(colU2, ni));
+      return (mode == 0) || (mode == 1 && u) || (mode == 2 && !u);
+    };
+#pragma unroll
+    for (int kk = 0; kk < kPB / 4; kk++) {
+      double2 b[NI];
+#pragma unroll
+      for (int ni = 0; ni < NI; ni++)
+        b[ni] = sh.op.B[swzB<BN>(kk * 4 + (t.lane & 3), t.wc * Tile::WC + ni * 8 + (t.lane >> 2))];
+#pragma unroll
+      for (int mi = 0; mi < MI; mi++) {
+        const double ax = sh.op.A[swzA(t.wr * Tile::WR + mi * 8 + (t.lane >> 2), kk * 4 + (t.lane & 3))].x;
+#pragma unroll
+        for (int ni = 0; ni < NI; ni++)
+          if (sel(mi, ni)) {
+            dmma(t.acc[mi][ni][0], t.acc[mi][ni][1], ax, b[ni].x);
+            dmma(t.acc[mi][ni][2], t.acc[mi][ni][3], ax, b[ni].y);
+          }
+      }
+#pragma unroll
+      for (int mi = 0; mi < MI; mi++) {
+        const double ay = sh.op.A[swzA(t.wr * Tile::WR + mi * 8 + (t.lane >> 2), kk * 4 + (t.lane & 3))].y;
+#pragma unroll
+        for (int ni = 0; ni < NI; ni++)
+          if (sel(mi, ni)) {
+            dmma(t.acc[mi][ni][0], t.acc[mi][ni][1], -ay, b[ni].y);
+            dmma(t.acc[mi][ni][2], t.acc[mi][ni][3], ay, b[ni].x);
+          }
+      }
+    }
+  };
+  // the first pivot block of a slice -> djjbuf for the T-server (all its warps call it)
+  auto publish_djj = [&](int s1) {
+    const int w0 = (s1 % p.NB) * kPB;
+    const int jnn = min(kPB, p.N - w0);
+    int ok = 1;
+    if (t.lane == 0 && s1 >= p.NB) ok = wait_ge(p, sy.d_used, s1 - p.NB);  // previous slice's was loaded
+    ok = __shfl_sync(kFull, ok, 0);
+    if (ok) {
+#pragma unroll
+      for (int mi = 0; mi < MI; mi++)
+#pragma unroll
+        for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            if (!(bit(rowU, mi) && bit(colU, ni))) continue;
+            const int r = t.row(mi) - w0, c = t.col(ni, h) - w0;
+            const double2 v = (r < jnn && c < jnn) ? cmk(t.acc[mi][ni][h], t.acc[mi][ni][2 + h])
+                                                   : cmk(r == c ? 1.0 : 0.0, 0.0);
+            __stcg(p.djjbuf + r * kPB + c, v);
+          }
+    }
+    int lead;
+    const int n = pub_set(kSetDjj, s1, &lead);
+    const int all_ok = !bar_or(kBarDjj, n * 32, !ok);
+    if (warp == lead && t.lane == 0 && all_ok) {
+      __threadfence();
+      st_release(sy.d_flag, s1);
+    }
+  };
+  // the pivot rows (rowbuf) and columns (pcbuf) of step s1; the lead warp
+  // releases the flags after every publishing warp wrote
+  auto publish_glob = [&](int s1) {
+    const int w0 = (s1 % p.NB) * kPB;
+    const int jnn = min(kPB, p.N - w0);
+    const int par = s1 & 1;
+    int lead;
+    const int n = pub_set(kSetGlob, s1, &lead);
+    if (warp == lead && t.lane == 0) trace_ev(p, s1 - 1, kTrGlobEnter);
+    int ok = 1;
+    if (t.lane == 0 && s1 >= 2) {
+      if (any_r) ok &= wait_ge(p, sy.row_cons + par * p.TC + Cq, p.TR * (s1 >> 1));
+      if (any_c && ok) ok &= wait_ge(p, sy.pc_cons + par * p.TR + I, p.TC * (s1 >> 1));
+    }
+    ok = __shfl_sync(kFull, ok, 0);
+    if (ok) {
+      double2* rowb = p.rowbuf + ((size_t)par * p.TC + Cq) * (kPB * BN);
+      double2* pcb = p.pcbuf + ((size_t)par * p.TR + I) * (BM * kPB);
+#pragma unroll
+      for (int mi = 0; mi < MI; mi++)
+#pragma unroll
+        for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            const int i = t.row(mi), j = t.col(ni, h);
+            const double2 v = cmk(t.acc[mi][ni][h], t.acc[mi][ni][2 + h]);
+            if (bit(rowU, mi)) {
+              const int k = (int)(i - w0);
+              __stcg(rowb + k * BN + (int)(j - tc0), (k < jnn) ? v : cmk(0.0, 0.0));
+            }
+            if (bit(colU, ni)) {
+              const int k = (int)(j - w0);
+              double2 wv;
+              if (k >= jnn || i >= p.R) wv = cmk(0.0, 0.0);
+              else if (i >= w0 && i < w0 + jnn) wv = cmk((i - w0 == k) ? 1.0 : 0.0, 0.0);
+              else wv = cneg(v);
+              __stcg(pcb + swzA((int)(i - tr0), k), wv);
+            }
+          }
+    }
+    if (warp == lead && t.lane == 0) trace_ev(p, s1 - 1, kTrGlobStored);
+    const int all_ok = !bar_or(kBarPub, n * 32, !ok);
+    if (warp == lead && t.lane == 0 && all_ok) {  // an aborted publish never releases anything
+      __threadfence();
+      if (w0 >= tr0 && w0 < tr0 + BM) st_release(sy.row_flag + Cq, s1);
+      if (w0 >= tc0 && w0 < tc0 + BN) st_release(sy.pc_flag + I, s1);
+      trace_ev(p, s1 - 1, kTrMathPublished);
+    }
+  };
+  // blocks (J_s2,J_s2), (J_s2,J_s1), (J_s1,J_s2) of the current W, s2 = s1+1,
+  // for the T-server's Schur update of step s2.  Beyond the last pivot row
+  // the first block is padded with the identity and the others with zeros.
+  auto publish_srv = [&](int s1) {
+    const int s2 = s1 + 1;
+    const int w1 = (s1 % p.NB) * kPB, w2 = w1 + kPB;
+    const int jn2 = min(kPB, p.N - w2);
+    const int par = s2 & 1;
+    int lead;
+    const int n = pub_set(kSetSrv, s1, &lead);
+    if (warp == lead && t.lane == 0) trace_ev(p, s1 - 1, kTrSrvPubEnter);
+    int ok = 1;
+    if (t.lane == 0 && s2 >= 2) ok = wait_ge(p, sy.srv_cons + par, s2 >> 1);
+    ok = __shfl_sync(kFull, ok, 0);
+    if (ok) {
+      double2* sb = p.srvbuf + (size_t)par * 3 * kPB * kPB;
+#pragma unroll
+      for (int mi = 0; mi < MI; mi++)
+#pragma unroll
+        for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            const int i = t.row(mi), j = t.col(ni, h);
+            const double2 v = cmk(t.acc[mi][ni][h], t.acc[mi][ni][2 + h]);
+            const int r2 = (int)(i - w2), c2 = (int)(j - w2), r1 = (int)(i - w1), c1 = (int)(j - w1);
+            if (bit(rowU2, mi) && bit(colU2, ni))
+              __stcg(sb + r2 * kPB + c2, (r2 < jn2 && c2 < jn2) ? v : cmk(r2 == c2 ? 1.0 : 0.0, 0.0));
+            if (bit(rowU2, mi) && bit(colU, ni)) __stcg(sb + kPB * kPB + r2 * kPB + c1, (r2 < jn2) ? v : cmk(0.0, 0.0));
+            if (bit(rowU, mi) && bit(colU2, ni)) __stcg(sb + 2 * kPB * kPB + r1 * kPB + c2, (c2 < jn2) ? v : cmk(0.0, 0.0));
+          }
+    }
+    if (warp == lead && t.lane == 0) trace_ev(p, s1 - 1, kTrSrvPubStored);
+    const int all_ok = !bar_or(kBarSrv, n * 32, !ok);
+    if (warp == lead && t.lane == 0 && all_ok) {
+      __threadfence();
+      const bool rin1 = w1 >= tr0 && w1 < tr0 + BM, rin2 = w2 >= tr0 && w2 < tr0 + BM;
+      const bool cin1 = w1 >= tc0 && w1 < tc0 + BN, cin2 = w2 >= tc0 && w2 < tc0 + BN;
+      int* f = sy.srv_flag + par * 3;
+      if (rin2 && cin2) st_release(f + 0, s2);
+      if (rin2 && cin1) st_release(f + 1, s2);
+      if (rin1 && cin2) st_release(f + 2, s2);
+      trace_ev(p, s1 - 1, kTrSrvPubDone);
+    }
+  };
+  // every piece this warp holds at the start of a slice (kernel start, or
+  // after the slice assembly): the first pivot block for the T-server, the
+  // first pivot rows / columns, and the server blocks of the second step
+  auto publish_start = [&](int s1) {
+    const bool with_srv = p.NB >= 2;
+    set_urgency(s1, with_srv);
+    if (any_r && any_c) publish_djj(s1);
+    if (any_r || any_c) publish_glob(s1);
+    if (any_srv) publish_srv(s1);
+  };
+
+  load_tile();
+  bar_sync(kBarMath, kMathThreads);
+  publish_start(0);
+
+  double probe_max = 0.0;
+  for (int s = 0; s < S; s++) {
+    const int n = s / p.NB, k = s % p.NB;
+    const int j0 = k * kPB, jn = min(kPB, p.N - j0);
+    const int par = s & 1;
+    // ---- operands of step s -> shared memory (TMA bulk copies) ----
+    bar_sync(kBarMath, kMathThreads);  // all warps are done with the previous tiles
+    if (warp == 0) {
+      if (t.lane == 0) trace_ev(p, s, kTrMathStart);
+      const bool ok = warp_wait_all(p, sy.u_flag + Cq * p.TR, p.TR, sy.pc_flag + I, s);
+      if (t.lane == 0) {
+        sh.math_abort = !ok;
+        trace_ev(p, s, kTrMathOperands);
+        if (ok) {
+          asm volatile("fence.proxy.async.global;" ::: "memory");
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          const uint32_t bytesA = BM * kPB * sizeof(double2), bytesB = kPB * BN * sizeof(double2);
+          const uint32_t mb = smem_u32(&sh.mbar);
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytesA + bytesB)
+                       : "memory");
+          const double2* srcA = p.pcbuf + ((size_t)par * p.TR + I) * (BM * kPB);
+          const double2* srcB = p.ubuf + ((size_t)par * p.TC + Cq) * (kPB * BN);
+          asm volatile(
+              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                  smem_u32(sh.op.A)),
+              "l"(srcA), "r"(bytesA), "r"(mb)
+              : "memory");
+          asm volatile(
+              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                  smem_u32(sh.op.B)),
+              "l"(srcB), "r"(bytesB), "r"(mb)
+              : "memory");
+        }
+      }
+    }
+    bar_sync(kBarMath, kMathThreads);
+    if (sh.math_abort) return;
+    {
+      const uint32_t mb = smem_u32(&sh.mbar);
+      uint32_t done = 0;
+      const long long t0 = clock64();
+      int timed_out = 0;
+      while (!done && !timed_out) {
+        asm volatile(
+            "{ .reg .pred P; mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2; selp.u32 %0, 1, 0, P; }"
+            : "=r"(done)
+            : "r"(mb), "r"((uint32_t)par)
+            : "memory");
+        if (!done && clock64() - t0 > p.timeout_cycles) timed_out = 1;
+      }
+      if (bar_or(kBarMath, kMathThreads, timed_out)) {
+        // the copies of this step may still be in flight: give them the same
+        // budget once more before the shared memory is abandoned
+        if (!done) {
+          const long long t1 = clock64();
+          while (!done && clock64() - t1 <= p.timeout_cycles)
+            asm volatile(
+                "{ .reg .pred P; mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2; selp.u32 %0, 1, 0, P; }"
+                : "=r"(done)
+                : "r"(mb), "r"((uint32_t)par)
+                : "memory");
+        }
+        if (tid == 0) {
+          atomicOr(p.status, kStatusTimeout);
+          atomicExch(p.abort, 1);
+        }
+        return;
+      }
+    }
+    if (tid == 0) {
+      trace_ev(p, s, kTrMathCopied);
+      atomicAdd(sy.pc_cons + par * p.TR + I, 1);
+      atomicAdd(sy.u_cons + par * p.TC + Cq, 1);
+    }
+    // ---- W_mod: rows and columns of the pivot block J read as zero ----
+#pragma unroll
+    for (int mi = 0; mi < MI; mi++)
+#pragma unroll
+      for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int i = t.row(mi), j = t.col(ni, h);
+          if ((i >= j0 && i < j0 + jn) || (j >= j0 && j < j0 + jn)) {
+            t.acc[mi][ni][h] = 0.0;
+            t.acc[mi][ni][2 + h] = 0.0;
+          }
+        }
+    // ---- rank-32 update; pieces of later steps first ----
+    const int s1 = s + 1;
+    const bool last_block = (k == p.NB - 1);
+    const bool slice_end = last_block && (s1 < S);
+    if (last_block) {
+      clear_urgency();
+    } else {
+      const bool with_srv = (k + 2 <= p.NB - 1);  // step s1 + 1 is in this slice
+      set_urgency(s1, with_srv);
+    }
+    if (!any_urg) {
+      mma_pass(0);
+    } else {
+      mma_pass(1);
+      if (any_r || any_c) publish_glob(s1);
+      if (any_srv) publish_srv(s1);
+      mma_pass(2);
+    }
+    if (tid == 0) trace_ev(p, s, kTrMathDone);
+    if (last_block) {
+      // slice boundary: the tile goes to its home in W, the probe is checked
+      // and the next slice matrix A_{n+1} - G_n is assembled there with plain
+      // code (keeps the accumulator-resident loop free of spills), then the
+      // tile is reloaded and the first pieces of slice n+1 published.
+      store_tile();
+      bar_sync(kBarMath, kMathThreads);
+      const double2* eps_next = slice_end ? p.eps + (p.eps_first + (int64_t)(n + 1) * p.eps_step) * p.N : nullptr;
+      probe_max = fmax(probe_max, boundary_pass<BM, BN>(p, I, Cq, tid, kMathThreads, eps_next));
+      bar_sync(kBarMath, kMathThreads);
+      if (slice_end) {
+        load_tile();
+        publish_start(s1);
+      }
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1) probe_max = fmax(probe_max, __shfl_xor_sync(kFull, probe_max, off));
+  if (t.lane == 0 && probe_max > 0.0)
+    atomicMax(p.probe_max, (unsigned long long)__double_as_longlong(probe_max));
+}
+
+// ---------------------------------------------------------------------------
+// tile CTA, panel warpgroup: U_s(:, my columns) = T_s * W(J_s, my columns)
+// ---------------------------------------------------------------------------
+template <int BM, int BN>
+__device__ void panel_role(const PersistParams& p, Shared& sh, const Sync& sy, int I, int Cq) {
+  const int t = threadIdx.x - Cfg<BM, BN>::MathThreads;
+  const int lane = t & 31, warp = t >> 5;
+  const int S = p.L * p.NB;
+  const int per = (BN + p.TR - 1) / p.TR;  // my columns of U(Cq): [cs, cs + w)
+  const int cs = I * per;
+  const int w = max(0, min(per, BN - cs));
+  for (int s = 0; s < S; s++) {
+    const int k = s % p.NB;
+    const int j0 = k * kPB, jn = min(kPB, p.N - j0);
+    const int par = s & 1;
+    if (t == 0) {
+      trace_ev(p, s, kTrPanelStart);
+      int ok = wait_ge(p, sy.t_flag, s);
+      ok = ok && wait_ge(p, sy.row_flag + Cq, s);
+      sh.panel_abort = !ok;
+      trace_ev(p, s, kTrPanelUin);
+    }
+    bar_sync(kBarPanel, kPanelThreads);
+    if (sh.panel_abort) return;
+    const double2* tb = p.tbuf + (size_t)par * kPB * kPB;
+    for (int e = t; e < kPB * kPB; e += kPanelThreads) sh.T[e / kPB][e % kPB] = __ldcg(tb + e);
+    const double2* rows = p.rowbuf + ((size_t)par * p.TC + Cq) * (kPB * BN);
+    double2* ub = p.ubuf + ((size_t)par * p.TC + Cq) * (kPB * BN);
+    bool waited_u = false;
+    for (int cc = 0; cc < w; cc += kPB) {
+      const int wc = min(kPB, w - cc);
+      for (int e = t; e < kPB * kPB; e += kPanelThreads) {
+        const int q = e / kPB, c = e % kPB;
+        sh.Mr[q][c] = (c < wc) ? __ldcg(rows + q * BN + cs + cc + c) : cmk(0.0, 0.0);
+      }
+      bar_sync(kBarPanel, kPanelThreads);
+      if (!waited_u) {
+        if (t == 0) sh.panel_abort = (s >= 2) ? !wait_ge(p, sy.u_cons + par * p.TC + Cq, p.TR * (s >> 1)) : 0;
+        bar_sync(kBarPanel, kPanelThreads);
+        if (sh.panel_abort) return;
+        waited_u = true;
+      }
+      // warp w owns rows [8w, 8w+8), one m8n8k4 column tile of 8 at a time
+      // (T_s is padded with the identity and the pivot rows with zeros beyond jn)
+      const int r = warp * 8 + (lane >> 2);
+      for (int nt = 0; nt * 8 < wc; nt++) {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int kk = 0; kk < kPB / 4; kk++) {
+          const double2 a = sh.T[r][kk * 4 + (lane & 3)];
+          const double2 bb = sh.Mr[kk * 4 + (lane & 3)][nt * 8 + (lane >> 2)];
+          dmma(acc[0], acc[1], a.x, bb.x);
+          dmma(acc[2], acc[3], a.x, bb.y);
+          dmma(acc[0], acc[1], -a.y, bb.y);
+          dmma(acc[2], acc[3], a.y, bb.x);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int c = nt * 8 + (lane & 3) * 2 + h;
+          if (c >= wc) continue;
+          const int64_t gc = (int64_t)Cq * BN + cs + cc + c;
+          double2 v = cmk(acc[h], acc[2 + h]);
+          if (r >= jn || gc >= p.C) v = cmk(0.0, 0.0);
+          else if (gc >= j0 && gc < j0 + jn) v = sh.T[r][gc - j0];
+          __stcg(ub + swzB<BN>(r, cs + cc + c), v);
+        }
+      }
+      bar_sync(kBarPanel, kPanelThreads);
+    }
+    bar_sync(kBarPanel, kPanelThreads);  // every read of T and of the pivot rows is done
+    if (t == 0) {
+      atomicAdd(sy.t_cons + par, 1);
+      atomicAdd(sy.row_cons + par * p.TC + Cq, 1);
+      __threadfence();
+      st_release(sy.u_flag + Cq * p.TR + I, s);
+      trace_ev(p, s, kTrPanelUout);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// T-server CTA
+// ---------------------------------------------------------------------------
+// Gauss-Jordan inversion of the 32x32 pivot block with partial pivoting,
+// register resident: lane r of warp w holds row r, columns [NC*w, NC*w+NC)
+// (32/NC warps).  The pivot search is one redux.sync over single-precision
+// magnitudes packed with the lane index; every candidate lane forms its
+// reciprocal while the search runs and the winner's reaches the other warps
+// through shared memory together with the pivot column (one barrier per
+// pivot).  The update is branch-free.  Row interchanges are implicit:
+//     inv[pinv[r]][perm[c]] = a(r, c),   perm[q] = row chosen at step q.
+template <int NC>
+__device__ __forceinline__ void gj_block(const PersistParams& p, Shared& sh, double2 (&a)[NC], int jn, int t,
+                                         int bar_id) {
+  constexpr int kWarps = kPB / NC;
+  const int lane = t & 31, warp = t >> 5;
+  unsigned used = 0;
+  for (int q = 0; q < jn; q++) {
+    const int b = q & 1;
+    if (warp == q / NC) {
+      const int cq = q % NC;
+      double2 vq = a[0];
+#pragma unroll
+      for (int c = 1; c < NC; c++) vq = (c == cq) ? a[c] : vq;
+      const double2 dq = crecip(vq);  // speculative: used only if this lane wins
+      const float fx = (float)vq.x, fy = (float)vq.y;
+      const float mag = fx * fx + fy * fy;
+      const bool elig = (lane < jn) && !((used >> lane) & 1u);
+      const unsigned key = elig ? ((__float_as_uint(mag) & ~63u) | (unsigned)(32 - lane)) : 0u;
+      const unsigned best = __reduce_max_sync(kFull, key);
+      const int pv = 32 - (int)(best & 63u);
+      const double2 d = cmk(__shfl_sync(kFull, dq.x, pv), __shfl_sync(kFull, dq.y, pv));
+      sh.fcol[b][lane] = vq;
+      if (lane == 0) {
+        sh.piv[b] = pv;
+        sh.dpiv[b] = d;
+        sh.perm[q] = pv;
+        if ((best >> 6) == 0u || !isfinite(d.x) || !isfinite(d.y)) atomicOr(p.status, kStatusSingular);
+      }
+    }
+    bar_sync(bar_id, kWarps * 32);
+    const int pv = sh.piv[b];
+    const double2 f = sh.fcol[b][lane];
+    const double2 d = sh.dpiv[b];
+    used |= 1u << pv;
+    const bool me = (lane == pv);
+#pragma unroll
+    for (int c = 0; c < NC; c++) {
+      const bool isq = (warp * NC + c == q);
+      const double2 pr = cmk(__shfl_sync(kFull, a[c].x, pv), __shfl_sync(kFull, a[c].y, pv));
+      const double2 sp = isq ? d : cmul(pr, d);
+      const double2 base = isq ? cmk(0.0, 0.0) : a[c];
+      const double2 upd = csub(base, cmul(f, sp));
+      a[c] = me ? sp : upd;
+    }
+  }
+}
+
+// Cout = Cin + alpha * A B for padded 32x32 complex blocks in shared memory
+// (Cin may be Cout: every element is read and written by the same thread),
+// on the FP64 tensor cores; 8 warps, warp w computes rows [8 (w>>1), +8) and
+// columns [16 (w&1), +16).
+__device__ __forceinline__ void blk_gemm(const Blk& A, const Blk& B, const Blk* Cin, double alpha, Blk& Cout, int t) {
+  const int lane = t & 31, warp = t >> 5;
+  const int r = 8 * (warp >> 1) + (lane >> 2), cb = 16 * (warp & 1);
+  double acc[2][4];
+#pragma unroll
+  for (int n = 0; n < 2; n++)
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const double2 c0 = Cin ? (*Cin)[r][cb + 8 * n + (lane & 3) * 2 + h] : cmk(0.0, 0.0);
+      acc[n][h] = c0.x;
+      acc[n][2 + h] = c0.y;
+    }
+#pragma unroll
+  for (int kk = 0; kk < kPB / 4; kk++) {
+    const double2 a = A[8 * (warp >> 1) + (lane >> 2)][kk * 4 + (lane & 3)];
+    const double ax = alpha * a.x, ay = alpha * a.y;
+    double2 b[2];
+#pragma unroll
+    for (int n = 0; n < 2; n++) b[n] = B[kk * 4 + (lane & 3)][cb + 8 * n + (lane >> 2)];
+#pragma unroll
+    for (int n = 0; n < 2; n++) {
+      dmma(acc[n][0], acc[n][1], ax, b[n].x);
+      dmma(acc[n][2], acc[n][3], ax, b[n].y);
+    }
+#pragma unroll
+    for (int n = 0; n < 2; n++) {
+      dmma(acc[n][0], acc[n][1], -ay, b[n].y);
+      dmma(acc[n][2], acc[n][3], ay, b[n].x);
+    }
+  }
+#pragma unroll
+  for (int n = 0; n < 2; n++)
+#pragma unroll
+    for (int h = 0; h < 2; h++) Cout[r][cb + 8 * n + (lane & 3) * 2 + h] = cmk(acc[n][h], acc[n][2 + h]);
+}
+
+// the 8 math warps of the server CTA form and invert every pivot block one
+// step ahead of the bulk update
+__device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, int t) {
+  const int lane = t & 31, warp = t >> 5;
+  const int S = p.L * p.NB;
+  const int ntiles = p.TR * p.TC;
+  for (int s = 0; s < S; s++) {
+    const int k = s % p.NB;
+    const int jn = min(kPB, p.N - k * kPB);
+    const int par = s & 1;
+    if (t == 0) {
+      trace_ev(p, s, kTrPanelStart);
+      bool ok;
+      if (k == 0) {
+        ok = wait_ge(p, sy.d_flag, s);
+      } else {
+        const int* f = sy.srv_flag + par * 3;
+        ok = wait_ge(p, f + 0, s) && wait_ge(p, f + 1, s) && wait_ge(p, f + 2, s);
+      }
+      sh.panel_abort = !ok;
+      trace_ev(p, s, kTrPanelTin);
+    }
+    bar_sync(kBarMath, kServerThreads);
+    if (sh.panel_abort) return;
+    if (k == 0) {
+      for (int e = t; e < kPB * kPB; e += kServerThreads) sh.srv.a1[e / kPB][e % kPB] = __ldcg(p.djjbuf + e);
+    } else {
+      const double2* sb = p.srvbuf + (size_t)par * 3 * kPB * kPB;
+      for (int e = t; e < kPB * kPB; e += kServerThreads) {
+        sh.srv.a1[e / kPB][e % kPB] = __ldcg(sb + e);
+        sh.srv.a2[e / kPB][e % kPB] = __ldcg(sb + kPB * kPB + e);
+        sh.srv.a3[e / kPB][e % kPB] = __ldcg(sb + 2 * kPB * kPB + e);
+      }
+    }
+    if (t < kPB) sh.perm[t] = t;
+    bar_sync(kBarMath, kServerThreads);
+    if (t == 0) {
+      if (k == 0) st_release(sy.d_used, s);
+      atomicAdd(sy.srv_cons + par, 1);
+      trace_ev(p, s, kTrSrvLoaded);
+    }
+    if (k != 0) {  // W^{(s-1)}(J_s,J_s) = a1 - a2 T_{s-1} a3
+      blk_gemm(sh.srv.tprev, sh.srv.a3, nullptr, 1.0, sh.srv.v, t);
+      bar_sync(kBarMath, kServerThreads);
+      blk_gemm(sh.srv.a2, sh.srv.v, &sh.srv.a1, -1.0, sh.srv.a1, t);
+      bar_sync(kBarMath, kServerThreads);
+    }
+    if (t == 0) trace_ev(p, s, kTrSrvSchur);
+    double2 a[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) a[c] = sh.srv.a1[lane][warp * 4 + c];
+    gj_block<4>(p, sh, a, jn, t, kBarMath);
+    bar_sync(kBarMath, kServerThreads);
+    if (t == 0) trace_ev(p, s, kTrSrvGJ);
+    if (t < kPB) sh.pinv[sh.perm[t]] = t;
+    if (t == 0) sh.panel_abort = (s >= 2) ? !wait_ge(p, sy.t_cons + par, ntiles * (s >> 1)) : 0;
+    bar_sync(kBarMath, kServerThreads);
+    if (sh.panel_abort) return;
+    double2* tb = p.tbuf + (size_t)par * kPB * kPB;
+    const int rr = sh.pinv[lane];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const int cc = sh.perm[warp * 4 + c];
+      __stcg(tb + rr * kPB + cc, a[c]);
+      sh.srv.tprev[rr][cc] = a[c];
+    }
+    bar_sync(kBarMath, kServerThreads);
+    if (t == 0) {
+      __threadfence();
+      st_release(sy.t_flag, s);
+      trace_ev(p, s, kTrPanelTout);
+    }
+  }
+}
+
+template <int BM, int BN>
+__global__ void __launch_bounds__(Cfg<BM, BN>::Threads, 1) k_persist(PersistParams p) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Shared& sh = *reinterpret_cast<Shared*>(smem_raw);
+  const int I = blockIdx.x / p.TC, Cq = blockIdx.x % p.TC;
+  Sync sy(p);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&sh.mbar)) : "memory");
+    sh.math_abort = 0;
+    sh.panel_abort = 0;
+  }
+  __syncthreads();
+  const bool server = blockIdx.x == (unsigned)(p.TR * p.TC);
+  static_assert(Cfg<BM, BN>::MathThreads == kServerThreads, "the server uses the math warpgroups");
+  if (threadIdx.x < Cfg<BM, BN>::MathThreads) {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(Cfg<BM, BN>::MathRegs));
+    if (server) server_role(p, sh, sy, threadIdx.x);
+    else math_role<BM, BN>(p, sh, sy, I, Cq);
+  } else {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(Cfg<BM, BN>::PanelRegs));
+    if (!server) panel_role<BM, BN>(p, sh, sy, I, Cq);
+  }
+}
+
+}  // namespace
+
+size_t persist_smem_bytes() { return sizeof(Shared); }
+
+int persist_threads(int BM, int BN) {
+  if (BM == 96) return Cfg<96, 96>::Threads;
+  if (BM == 64) return Cfg<64, 64>::Threads;
+  return Cfg<32, 32>::Threads;
+}
+
+// tile shape: the largest that keeps >= 60% of the SMs busy, else the one
+// with the most CTAs; one SM always stays free for the T-server CTA
+bool persist_choose_tile(int64_t R, int64_t C, int sms, int* BM, int* BN) {
+  const int cand[3] = {96, 64, 32};
+  const int avail = sms - 1;
+  for (int q = 0; q < 3; q++) {
+    const int64_t tiles = ((R + cand[q] - 1) / cand[q]) * ((C + cand[q] - 1) / cand[q]);
+    if (tiles <= avail && tiles * 10 >= (int64_t)avail * 6) {
+      *BM = *BN = cand[q];
+      return true;
+    }
+  }
+  for (int q = 2; q >= 0; q--) {
+    const int64_t tiles = ((R + cand[q] - 1) / cand[q]) * ((C + cand[q] - 1) / cand[q]);
+    if (tiles <= avail) {
+      *BM = *BN = cand[q];
+      return true;
+    }
+  }
+  return false;
+}
+
+cudaError_t launch_persist(const PersistParams& p, int BM, int BN, cudaStream_t s) {
+  PersistParams pp = p;
+  void* args[] = {(void*)&pp};
+  const size_t smem = sizeof(Shared);
+  const void* fn = nullptr;
+  if (BM == 96 && BN == 96) fn = (const void*)k_persist<96, 96>;
+  else if (BM == 64 && BN == 64) fn = (const void*)k_persist<64, 64>;
+  else if (BM == 32 && BN == 32) fn = (const void*)k_persist<32, 32>;
+  else return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  return cudaLaunchCooperativeKernel(fn, dim3(p.TR * p.TC + 1), dim3(persist_threads(BM, BN)), args, smem, s);
+}
+
+}  // namespace rgf

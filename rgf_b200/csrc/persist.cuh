@@ -1,0 +1,55 @@
+// Persistent slice-recursion kernel (see persist.cu).
+#pragma once
+#include "rgf_internal.cuh"
+
+namespace rgf {
+
+struct PersistParams {
+  int N, R, C;           // pivot dimension, active rows, active columns of the augmented matrix
+  int TR, TC;            // tile grid (TR x TC CTAs)
+  int NB;                // pivot blocks per slice = ceil(N / 32)
+  int L;                 // slices swept by this launch
+  double2* M;            // augmented matrix (row-major, leading dimension ldm): in and out
+  int64_t ldm;
+  const double2* eps;    // slice n (recursion order) is eps + (eps_first + n * eps_step) * N
+  int64_t eps_first, eps_step;
+  double2 k2;            // k0dx^2
+  const int* st_col;     // A0 stencil, kMaxStencil entries per row
+  const double2* st_val;
+  int pc1;               // probe columns pc1, pc1 + 1 (pc1 even), -1 = none
+  double2* pcbuf;        // [2][TR][BM][32]
+  double2* rowbuf;       // [2][TC][32][BN]
+  double2* tbuf;         // [2][32][32]
+  double2* ubuf;         // [2][TC][32][BN]
+  double2* djjbuf;       // [32][32] first pivot block of a slice, for the T-server CTA
+  double2* srvbuf;       // [2][3][32][32] blocks the T-server updates into the next pivot block
+  int* flags;            // pc[TR], row[TC], t[1], u[TC*TR], d[1], srv[2][3], d_used[1]  (init -1)
+  int* cons;             // pc[2][TR], row[2][TC], t[2], u[2][TC], srv[2]             (init 0)
+  int* status;           // kStatus* bits
+  int* abort;            // raised by the first wait that times out
+  unsigned long long* probe_max;  // bits of max |G_n M_n v - v| (non-negative double)
+  long long timeout_cycles;
+  // optional per-step event timestamps (%globaltimer, ns) for the first
+  // trace_steps steps: trace[(cta * trace_steps + s) * kTraceEvents + e]
+  unsigned long long* trace;
+  int trace_steps;
+};
+
+// trace events: math role
+enum { kTrMathStart = 0, kTrMathOperands, kTrMathCopied, kTrMathPublished, kTrMathDone,
+       // panel role
+       kTrPanelStart, kTrPanelTin, kTrPanelTout, kTrPanelUin, kTrPanelUout,
+       // finer grain: server pieces loaded / next pivot block formed / GJ done
+       kTrSrvLoaded, kTrSrvSchur, kTrSrvGJ,
+       // publication of the pivot rows / columns and of the server blocks (lead warp)
+       kTrGlobEnter, kTrGlobStored, kTrSrvPubEnter, kTrSrvPubStored, kTrSrvPubDone, kTraceEvents };
+
+inline int persist_flag_words(int TR, int TC) { return TR + TC + 1 + TR * TC + 1 + 6 + 1; }
+inline int persist_cons_words(int TR, int TC) { return 2 * TR + 2 * TC + 2 + 2 * TC + 2; }
+
+size_t persist_smem_bytes();
+int persist_threads(int BM, int BN);
+bool persist_choose_tile(int64_t R, int64_t C, int sms, int* BM, int* BN);
+cudaError_t launch_persist(const PersistParams& p, int BM, int BN, cudaStream_t s);
+
+}  // namespace rgf

@@ -9,13 +9,18 @@
 // Input validation mirrors cal_smatrix_RGF.m:79-93 / 103-178; errors are
 // returned as rgf_status with a message in rgf_last_error().
 #include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
 #include <string>
+#include <chrono>
+#include <thread>
 #include <vector>
 
 #include "channels.cuh"
+#include "persist.cuh"
 #include "rgf_internal.cuh"
 #include "sweep.cuh"
 
@@ -44,7 +49,10 @@ struct rgf_handle_s {
   // workspace (grow-only)
   DevBuf k0, k1, kx[2], lam[2], mu[2], isprop[2], prop[2], conj[2], nprop, status;
   DevBuf phi, tmp, g0s, g0e, st_col, st_val, eps, aug, pc, u, idx, sdev;
+  DevBuf xpc, xrow, xt, xu, xsync, xprobe, xtrace;  // persistent-kernel exchange buffers
+  int sms = 0;
   int64_t launches = 0;
+  std::string prof_kernel;
   double probe = 0.0;
 };
 
@@ -378,7 +386,9 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
   const std::vector<int>& out_e = rq.out[e];
   const int ni_s = (int)in_s.size(), no_s = (int)out_s.size(), ni_e = (int)in_e.size(), no_e = (int)out_e.size();
   const int64_t R = N + no_s + no_e, C = N + ni_s + ni_e;
-  const int64_t ldm = (C + 1) & ~(int64_t)1;
+  // persistent engine: active R_p x C_p with the probe pair at an even column
+  const int64_t Rp = N + no_s, pc1 = (N + ni_s + 1) & ~(int64_t)1, Cp = pc1 + 2;
+  const int64_t ldm = (std::max(C, Cp) + 1) & ~(int64_t)1;
   const int kSwW = sweep_block_width();
 
   // (3) workspace
@@ -389,7 +399,7 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
   if ((st = ensure(h->st_col, sizeof(int) * N * kMaxStencil))) return st;
   if ((st = ensure(h->st_val, sizeof(double2) * N * kMaxStencil))) return st;
   if ((st = ensure(h->aug, sizeof(double2) * R * ldm))) return st;
-  if ((st = ensure(h->pc, sizeof(double2) * R * kSwW))) return st;
+  if ((st = ensure(h->pc, sizeof(double2) * std::max(R, Cp) * kSwW))) return st;
   if ((st = ensure(h->u, sizeof(double2) * kSwW * ldm))) return st;
   if ((st = ensure(h->status, sizeof(int)))) return st;
   if (!S_dev && (st = ensure(h->sdev, sizeof(double2) * (int64_t)n_out * n_in))) return st;
@@ -515,7 +525,154 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
     }
     return RGF_OK;
   };
-  for (int64_t k = 0; k < L; k++) {
+  int BMp = 0, BNp = 0;
+  bool use_persist = L > 0 && !(opt && opt->engine == 1) && persist_choose_tile(Rp, Cp, h->sms, &BMp, &BNp);
+  unsigned long long* probe_d = nullptr;
+  h->prof_kernel = sweep_update_kernel_name();
+  if (use_persist) {
+    const int TR = (int)((Rp + BMp - 1) / BMp), TC = (int)((Cp + BNp - 1) / BNp);
+    const int nflags = persist_flag_words(TR, TC), ncons = persist_cons_words(TR, TC);
+    if ((st = ensure(h->xpc, sizeof(double2) * 2 * TR * BMp * 32))) return st;
+    if ((st = ensure(h->xrow, sizeof(double2) * 2 * TC * 32 * BNp))) return st;
+    if ((st = ensure(h->xt, sizeof(double2) * 9 * 32 * 32))) return st;  // tbuf[2], djjbuf, srvbuf[2][3]
+    if ((st = ensure(h->xu, sizeof(double2) * 2 * TC * 32 * BNp))) return st;
+    if ((st = ensure(h->xsync, sizeof(int) * (nflags + ncons + 4)))) return st;
+    if ((st = ensure(h->xprobe, sizeof(unsigned long long)))) return st;
+    int* flags = as<int>(h->xsync);
+    RGF_CUDA_TRY(cudaMemsetAsync(flags, 0xFF, sizeof(int) * nflags, h->stream));
+    RGF_CUDA_TRY(cudaMemsetAsync(flags + nflags, 0, sizeof(int) * (ncons + 4), h->stream));
+    probe_d = as<unsigned long long>(h->xprobe);
+    RGF_CUDA_TRY(cudaMemsetAsync(probe_d, 0, sizeof(unsigned long long), h->stream));
+    launch_probe_init(M, ldm, N, Rp, pc1, h->stream);
+    h->launches++;
+    PersistParams pp;
+    pp.N = (int)N;
+    pp.R = (int)Rp;
+    pp.C = (int)Cp;
+    pp.TR = TR;
+    pp.TC = TC;
+    pp.NB = (int)((N + kSwW - 1) / kSwW);
+    pp.L = (int)L;
+    pp.M = M;
+    pp.ldm = ldm;
+    pp.eps = eps_d;
+    pp.eps_first = mirror ? L - 1 : 0;
+    pp.eps_step = mirror ? -1 : 1;
+    pp.k2 = k2;
+    pp.st_col = st_col;
+    pp.st_val = st_val;
+    pp.pc1 = (int)pc1;
+    pp.pcbuf = as<double2>(h->xpc);
+    pp.rowbuf = as<double2>(h->xrow);
+    pp.tbuf = as<double2>(h->xt);
+    pp.djjbuf = as<double2>(h->xt) + 2 * 32 * 32;
+    pp.srvbuf = as<double2>(h->xt) + 3 * 32 * 32;
+    pp.ubuf = as<double2>(h->xu);
+    pp.flags = flags;
+    pp.cons = flags + nflags;
+    pp.abort = flags + nflags + ncons;
+    pp.status = status;
+    pp.probe_max = probe_d;
+    int clk_khz = 2000000;
+    cudaDeviceGetAttribute(&clk_khz, cudaDevAttrClockRate, h->device);
+    pp.timeout_cycles = (long long)clk_khz * 1000LL * 4;  // ~4 s per wait
+    // RGF_TRACE=<file>: record per-step role timestamps of the first
+    // RGF_TRACE_STEPS (default 128) steps.  RGF_WATCH=<seconds> (with
+    // RGF_TRACE): if the launch is still running after that long, the trace
+    // recorded so far is read through a second stream and written, and the
+    // call fails with RGF_ERR_TIMEOUT.
+    const char* trace_path = getenv("RGF_TRACE");
+    const char* watch_env = getenv("RGF_WATCH");
+    const char* steps_env = getenv("RGF_TRACE_STEPS");
+    pp.trace = nullptr;
+    pp.trace_steps = 0;
+    if (trace_path && *trace_path) {
+      pp.trace_steps = steps_env ? std::max(1, std::min(atoi(steps_env), (int)(L * pp.NB))) : 128;
+      if ((st = ensure(h->xtrace, sizeof(unsigned long long) * (size_t)(TR * TC + 1) * pp.trace_steps * kTraceEvents)))
+        return st;
+      pp.trace = as<unsigned long long>(h->xtrace);
+      RGF_CUDA_TRY(cudaMemsetAsync(pp.trace, 0, h->xtrace.bytes, h->stream));
+    }
+    const bool timed = prof_every > 0;
+    if (timed) {
+      while (h->ev.size() < 2) {
+        cudaEvent_t ev;
+        RGF_CUDA_TRY(cudaEventCreate(&ev));
+        h->ev.push_back(ev);
+      }
+      RGF_CUDA_TRY(cudaEventRecord(h->ev[0], h->stream));
+    }
+    cudaError_t e = launch_persist(pp, BMp, BNp, h->stream);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      use_persist = false;  // e.g. the cooperative launch does not fit: per-step engine below
+      probe_d = nullptr;
+    } else {
+      h->launches++;
+      if (timed) {
+        RGF_CUDA_TRY(cudaEventRecord(h->ev[1], h->stream));
+        ev_used = 2;
+        for (int64_t j0 = 0; j0 < N; j0 += kSwW)
+          prof_flops += (double)L * 8.0 * (double)Rp * (double)(N + ni_s) * (double)std::min<int64_t>(kSwW, N - j0);
+      }
+      char nm[64];
+      snprintf(nm, sizeof(nm), "k_persist<%d,%d> (FP64 DMMA sweep, all slices)", BMp, BNp);
+      h->prof_kernel = nm;
+      bool hung = false;
+      if (pp.trace && watch_env && atof(watch_env) > 0) {
+        const auto t_start = std::chrono::steady_clock::now();
+        for (;;) {
+          const cudaError_t q = cudaStreamQuery(h->stream);
+          if (q == cudaSuccess) break;
+          if (q != cudaErrorNotReady) RGF_CUDA_TRY(q);
+          const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+          if (el > atof(watch_env)) {
+            hung = true;
+            break;
+          }
+          std::this_thread::sleep_for(std::chrono::milliseconds(10));
+        }
+      }
+      if (pp.trace) {
+        std::vector<unsigned long long> tr((size_t)(TR * TC + 1) * pp.trace_steps * kTraceEvents);
+        if (hung) {
+          cudaStream_t side;
+          RGF_CUDA_TRY(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+          RGF_CUDA_TRY(cudaMemcpyAsync(tr.data(), pp.trace, sizeof(unsigned long long) * tr.size(),
+                                       cudaMemcpyDeviceToHost, side));
+          std::vector<int> words(nflags + ncons + 1);
+          RGF_CUDA_TRY(cudaMemcpyAsync(words.data(), flags, sizeof(int) * words.size(), cudaMemcpyDeviceToHost, side));
+          RGF_CUDA_TRY(cudaStreamSynchronize(side));
+          const std::string wpath = std::string(trace_path) + ".flags";
+          if (FILE* fw = fopen(wpath.c_str(), "wb")) {
+            fwrite(words.data(), sizeof(int), words.size(), fw);
+            fclose(fw);
+          }
+          FILE* f = fopen(trace_path, "wb");
+          if (f) {
+            int hdr[4] = {TR, TC, pp.trace_steps, (int)kTraceEvents};
+            fwrite(hdr, sizeof(int), 4, f);
+            fwrite(tr.data(), sizeof(unsigned long long), tr.size(), f);
+            fclose(f);
+          }
+          set_error("persistent sweep still running after RGF_WATCH seconds; trace written");
+          return RGF_ERR_TIMEOUT;
+        }
+        RGF_CUDA_TRY(cudaMemcpyAsync(tr.data(), pp.trace, sizeof(unsigned long long) * tr.size(),
+                                     cudaMemcpyDeviceToHost, h->stream));
+        RGF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        FILE* f = fopen(trace_path, "wb");
+        if (f) {
+          int hdr[4] = {TR, TC, pp.trace_steps, (int)kTraceEvents};
+          fwrite(hdr, sizeof(int), 4, f);
+          fwrite(tr.data(), sizeof(unsigned long long), tr.size(), f);
+          fclose(f);
+        }
+      }
+      attach(false);
+    }
+  }
+  for (int64_t k = 0; !use_persist && k < L; k++) {
     if ((st = sweep(N + no_s, N + ni_s, prof_every && (k % prof_every) == 0))) return st;
     if (k + 1 < L) {
       launch_assemble(M, ldm, N, N + no_s, M, ldm, nullptr, 0, st_col, st_val, k2, slice_eps(k + 1), cmk(0, 0),
@@ -540,8 +697,12 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
                                    sizeof(double2) * n_out, n_in, cudaMemcpyDeviceToHost, h->stream));
   }
   int hstatus = 0;
+  unsigned long long probe_bits = 0;
   RGF_CUDA_TRY(cudaMemcpyAsync(&hstatus, status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  if (probe_d)
+    RGF_CUDA_TRY(cudaMemcpyAsync(&probe_bits, probe_d, sizeof(probe_bits), cudaMemcpyDeviceToHost, h->stream));
   RGF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  memcpy(&h->probe, &probe_bits, sizeof(double));
   h->prof_n = (int64_t)(ev_used / 2);
   h->prof_ms = 0.0;
   h->prof_flops = prof_flops;
@@ -639,6 +800,7 @@ rgf_status rgf_create(int device, rgf_handle* out) {
     return RGF_ERR_CUDA;
   }
   h->stream = h->own_stream;
+  cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, device);
   *out = h;
   return RGF_OK;
 }
@@ -650,7 +812,8 @@ rgf_status rgf_destroy(rgf_handle h) {
                     &h->mu[0],  &h->mu[1],  &h->isprop[0], &h->isprop[1], &h->prop[0], &h->prop[1],
                     &h->conj[0], &h->conj[1], &h->nprop,   &h->status,    &h->phi,     &h->tmp,
                     &h->g0s,    &h->g0e,    &h->st_col,    &h->st_val,    &h->eps,     &h->aug,
-                    &h->pc,     &h->u,      &h->idx,       &h->sdev};
+                    &h->pc,     &h->u,      &h->idx,       &h->sdev,      &h->xpc,     &h->xrow,
+                    &h->xt,     &h->xu,     &h->xsync,     &h->xprobe,    &h->xtrace};
   for (DevBuf* b : bufs)
     if (b->p) cudaFree(b->p);
   for (cudaEvent_t ev : h->ev) cudaEventDestroy(ev);
@@ -783,7 +946,7 @@ rgf_status rgf_last_profile(rgf_handle h, int64_t* timed_launches, double* total
   if (total_ms) *total_ms = h->prof_ms;
   if (flops_per_launch) *flops_per_launch = h->prof_n ? h->prof_flops / (double)h->prof_n : 0.0;
   if (kernel_name && name_len) {
-    strncpy(kernel_name, sweep_update_kernel_name(), name_len - 1);
+    strncpy(kernel_name, h->prof_kernel.c_str(), name_len - 1);
     kernel_name[name_len - 1] = 0;
   }
   return RGF_OK;

@@ -34,6 +34,16 @@ __host__ __device__ inline double2 cinv(double2 a) {
   }
 }
 
+// probe vector of the a-posteriori slice-inverse check:
+// v(i) = exp(2 pi i frac(i * golden ratio)), |v(i)| = 1
+__device__ inline double2 probe_v(int64_t i) {
+  double f = (double)i * 0.6180339887498949;
+  f -= floor(f);
+  double s, c;
+  sincospi(2.0 * f, &s, &c);
+  return make_double2(c, s);
+}
+
 // ---------------------------------------------------------------------------
 // problem description shared by the host orchestrator and the kernels
 // ---------------------------------------------------------------------------

@@ -420,6 +420,31 @@ void launch_extract(const double2* M, int64_t ldm, int64_t N, const int* row_of,
 }
 
 // ---------------------------------------------------------------------------
+// probe columns of the first slice: p1 = v, p2 = M_1 v (top-left block of the
+// assembled matrix times v), rows [N, R) zero.  One warp per row.
+// ---------------------------------------------------------------------------
+__global__ void k_probe_init(double2* M, int64_t ldm, int64_t N, int64_t R, int64_t pc1) {
+  const int64_t i = blockIdx.x * (int64_t)(blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (i >= R) return;
+  double2 acc = cmk(0.0, 0.0);
+  if (i < N)
+    for (int64_t j = lane; j < N; j += 32) acc = cadd(acc, cmul(M[i * ldm + j], probe_v(j)));
+  for (int off = 16; off > 0; off >>= 1) {
+    acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
+    acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
+  }
+  if (lane == 0) {
+    M[i * ldm + pc1] = (i < N) ? probe_v(i) : cmk(0.0, 0.0);
+    M[i * ldm + pc1 + 1] = (i < N) ? acc : cmk(0.0, 0.0);
+  }
+}
+
+void launch_probe_init(double2* M, int64_t ldm, int64_t N, int64_t R, int64_t pc1, cudaStream_t s) {
+  k_probe_init<<<(unsigned)((R + 7) / 8), 256, 0, s>>>(M, ldm, N, R, pc1);
+}
+
+// ---------------------------------------------------------------------------
 // misc
 // ---------------------------------------------------------------------------
 __global__ void k_check_finite(const double2* x, int64_t n, int* status) {

@@ -31,6 +31,7 @@ void launch_fill_attach(double2* M, int64_t ldm, int64_t N, int ni_s, int no_s, 
                         const int* out_e, int no_e, cudaStream_t s);
 void launch_extract(const double2* M, int64_t ldm, int64_t N, const int* row_of, int no, const int* col_of,
                     int ni, double2* S, int64_t ldS, const int* pairs, int npairs, cudaStream_t s);
+void launch_probe_init(double2* M, int64_t ldm, int64_t N, int64_t R, int64_t pc1, cudaStream_t s);
 void launch_check_finite(const double2* x, int64_t n, int* status, cudaStream_t s);
 void launch_scale_cols(const double2* src, int64_t lds, const double2* diag, double2* dst, int64_t ldd,
                        int64_t rows, int64_t cols, cudaStream_t s);

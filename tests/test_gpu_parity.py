@@ -149,3 +149,21 @@ def test_repeated_calls_reuse_workspace():
     for case in (a, b, a):
         S, _ = run(case)
         assert rel(S, case["S"]) <= TOL_S
+
+
+@pytest.mark.parametrize("name", ["cfg1", "cfg5", "2d_large_N_gt_block", "3d_bloch_inR", "2d_Bloch_inL"])
+def test_engines_agree_and_probe(name):
+    """The persistent register-resident engine (default) and the per-step
+    engine give the same S; the per-slice probe residual max|G_n M_n v - v|
+    stays at round-off level."""
+    case = config_case(name) if name.startswith("cfg") else load_case(os.path.join(GOLDEN, name + ".npz"))
+    h = _abi.Handle(0)
+    fn = rgf_b200.cal_smatrix_RGF if case["dim"] == "2d" else rgf_b200.cal_smatrix_RGF_3D
+    S0, _ = fn(case["syst"], case["out"], case["in"], handle=h, options={"engine": 0})
+    launches0, probe = h.stats()
+    S1, _ = fn(case["syst"], case["out"], case["in"], handle=h, options={"engine": 1})
+    launches1, _ = h.stats()
+    assert rel(S0, case["S"]) <= TOL_S and rel(S1, case["S"]) <= TOL_S
+    assert rel(S0, S1) <= 1e-12
+    assert probe < 1e-10
+    assert launches0 < launches1
