@@ -11,9 +11,12 @@ A step is one full S-matrix (204 x 204) of the config-2 structure.
            (256 MiB write) between steps, max over ranks.
 * e2e    : the same through the C ABI with pinned HOST epsilon and S; the
            timed region includes the 64 MiB H2D of epsilon and the D2H of S.
-* roofline: the dominant kernel (the sweep's rank-32 FP64 DMMA update),
-           sampled with CUDA events every 64th slice; peak = FP64 DMMA rate
-           measured on this pool's B200s (profiles/fp64_dmma_peak.md).
+* roofline: the dominant kernel (the persistent FP64 DMMA sweep, one launch
+           per S-matrix covering all L slices), timed with CUDA events on the
+           library's stream; achieved = canonical flops of the L slices
+           (8N^3 + 8N^2(P_in+P_out) + 8N P_out P_in per slice) / launch time;
+           peak = the FP64 mma.sync rate measured in this same run by
+           librgf_peak.so (the driver's peaks file has no FP64 figure).
 * cpu_baseline: the numpy/scipy oracle (restatement of the MATLAB reference;
            MATLAB itself is not installed) on the host cores, on a bounded
            sample of slices, extrapolated linearly in L.
@@ -41,7 +44,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "S-matrices/s 2D N=1024 L=4096: 3xTF32+refine vs FP64 at 1e-10 rel err; grad/fwd"
 UNIT = "S-matrices/s"
-FP64_DMMA_PEAK_TFLOPS = 37.0  # measured on this pool, profiles/fp64_dmma_peak.md
+FP64_DMMA_FALLBACK_TFLOPS = 37.0  # earlier measurement on this pool, used only if the live one fails
 PROFILE_EVERY = 64
 
 
@@ -183,6 +186,23 @@ def run_reference(args, dist):
     print(json.dumps(line), flush=True)
 
 
+def measure_fp64_peak(device: int):
+    """FP64 tensor-core rate measured now on this GPU (librgf_peak.so):
+    returns (best DMMA TFLOP/s, source text)."""
+    from rgf_b200 import build
+    try:
+        lib = ctypes.CDLL(str(build.PEAK_OUT))
+        out = (ctypes.c_double * 3)()
+        rc = lib.rgf_peak_fp64(ctypes.c_int(device), out)
+        if rc == 0 and out[0] > 0:
+            best = max(out[0], out[1])
+            return best, (f"FP64 mma.sync rate measured in this run (librgf_peak.so): m8n8k4 {out[0]:.2f}, "
+                          f"m16n8k16 {out[1]:.2f}, DFMA {out[2]:.2f} TFLOP/s; peak = best DMMA (burst)")
+    except OSError:
+        pass
+    return FP64_DMMA_FALLBACK_TFLOPS, "fallback: earlier FP64 DMMA measurement on this pool (37 TFLOP/s)"
+
+
 def config_dict():
     return {"workload": "config2: 2D Dirichlet, N=1024 transverse sites, L=4096 slices, eps 2.25 + 30% disks "
                         "(r 4-12 px) of 1 + 1j*U[0,0.01), k0dx=2pi/20, full S (P=102 per side, 204x204)",
@@ -249,6 +269,7 @@ def run_ours(args, dist):
                 prof[3] = name
         return total_ms, prof
 
+    peak, peak_source = measure_fp64_peak(dev)
     for _ in range(args.warmup):
         step(True, 0)
     torch.cuda.synchronize()
@@ -283,17 +304,17 @@ def run_ours(args, dist):
     line["canonical_tflops"] = F * value / 1e12 / dist.world
     line["precision_form"] = None
     line["grad_over_fwd"] = None
-    n, ms, fl, name = prof
+    n, ms, fl_exec, name = prof
+    fl = nx * workloads.canonical_slice_flops(ny, n_in // 2, n_out // 2)  # the launch covers all nx slices
     achieved = fl / (ms / n / 1e3) / 1e12 if n else None
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         traffic = json.load(open(tpath)).get("sweep_update_bytes_per_launch")
-    line["roofline"] = {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": FP64_DMMA_PEAK_TFLOPS,
-                        "unit": "TFLOP/s", "frac": (achieved / FP64_DMMA_PEAK_TFLOPS) if achieved else None,
-                        "traffic": traffic, "flops_per_launch": fl, "timed_launches": n,
-                        "peak_source": "FP64 DMMA (mma.sync f64) microbenchmark on this pool's B200, burst "
-                                       "(MEASURED_PEAKS.json has no FP64 figure)"}
+    line["roofline"] = {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": peak,
+                        "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
+                        "traffic": traffic, "flops_per_launch": fl, "executed_flops_per_launch": fl_exec,
+                        "timed_launches": n, "peak_source": peak_source}
     line["e2e"] = {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(eps_host.numel() * 16),
                    "d2h_bytes_per_step": int(n_out * n_in * 16)}
     line["gpu_launches"] = int(launches) * args.steps

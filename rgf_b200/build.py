@@ -2,7 +2,8 @@
 
 The shared library is built in-tree (``rgf_b200/librgf.so``) with nvcc,
 statically linked against the CUDA runtime so it loads without touching
-torch's bundled runtime.
+torch's bundled runtime.  ``librgf_peak.so`` (the FP64 peak microbenchmark
+bench.py uses as its roofline denominator) is built beside it.
 """
 from __future__ import annotations
 
@@ -14,6 +15,7 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 OUT = PKG / "librgf.so"
+PEAK_OUT = PKG / "librgf_peak.so"
 SOURCES = ["channels.cu", "sweep.cu", "persist.cu", "rgf_api.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
@@ -33,6 +35,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     if OUT.exists() and not force:
         newest = max(p.stat().st_mtime for p in deps)
         if OUT.stat().st_mtime >= newest:
+            build_peak(verbose, force)
             return OUT
     objdir = PKG / "_build"
     objdir.mkdir(exist_ok=True)
@@ -50,7 +53,21 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
     os.replace(tmp, OUT)
+    build_peak(verbose, force)
     return OUT
+
+
+def build_peak(verbose: bool = False, force: bool = False) -> Path:
+    src = CSRC / "peak.cu"
+    if PEAK_OUT.exists() and not force and PEAK_OUT.stat().st_mtime >= src.stat().st_mtime:
+        return PEAK_OUT
+    tmp = PEAK_OUT.with_suffix(".so.tmp")
+    cmd = [nvcc(), *ARCH, *FLAGS, "-shared", "-cudart", "static", "-o", str(tmp), str(src)]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, PEAK_OUT)
+    return PEAK_OUT
 
 
 if __name__ == "__main__":

@@ -91,6 +91,13 @@ def config5(seed: int = 5, ny: int = 256, nx: int = 512):
     return syst, {"ind_out_R": np.arange(1, 9)}, {"ind_in_L": np.arange(1, 9)}
 
 
+def canonical_slice_flops(N: int, pin: int, pout: int) -> float:
+    """Channel-projected algorithmic flops of one slice of the recursion:
+    inverse 8N^3, carriers X = G B_L and Z = C_L G (8N^2 each per channel),
+    Y += Z X (8N P_out P_in); pin / pout are the left-side channel counts."""
+    return 8.0 * N ** 3 + 8.0 * N * N * (pin + pout) + 8.0 * N * pout * pin
+
+
 def canonical_flops(N: int, L: int, pin: int, pout: int, distinct_leads: bool = False) -> float:
     """Channel-projected algorithmic flop count of one S-matrix (real flops,
     complex multiply-add = 8): per slice 8N^3 (inverse) + 8N^2 (P_in + P_out)
