@@ -185,6 +185,35 @@ RGF_API rgf_status rgf_last_profile(rgf_handle h, int64_t* timed_launches, doubl
  * NULL restores the handle's own stream. */
 RGF_API rgf_status rgf_set_stream(rgf_handle h, void* stream);
 
+/* ---- allocation-free variant -------------------------------------------------
+ * No counterpart in the reference: an addition of this library.
+ *
+ * rgf_smatrix_2d without a handle and without any device allocation, for
+ * callers that must not call cudaMalloc/cudaFree: code that runs inside a
+ * host application owning the device memory pool (MATLAB's gpuArray memory
+ * manager, a deep-learning framework's caching allocator), where a library
+ * allocating on its own would fail once the pool has claimed the memory or
+ * fragment it, and latency-bound callers for which cudaMalloc/cudaFree, which
+ * can synchronize the whole device, are not acceptable.  The caller still
+ * passes every input and output (syst, req, S, ch as for rgf_smatrix_2d); all
+ * device workspace -- channel data, the augmented slice matrix, the sweep's
+ * exchange buffers and flags -- is carved from one static device array of
+ * RGF_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
+ * the process exits.  A problem whose workspace does not fit is rejected with
+ * RGF_ERR_ARG and a message naming the limit (roughly: 16 bytes times
+ * (N + n_out)(N + n_in + 2) for the slice matrix, plus N*L*16 when epsilon is
+ * on the host, plus a few N-sized arrays, N = ny).  Work is issued on
+ * `stream` (a cudaStream_t; NULL = the legacy default stream) of the current
+ * device.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  Every call on a device shares the one array,
+ * so calls that overlap on the GPU (other host threads, other streams) race;
+ * each call clears what must start at zero.  opt->profile must be 0. */
+#define RGF_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
+RGF_API rgf_status rgf_smatrix_2d_noalloc(const rgf_syst2d* syst, const rgf_request* req,
+                                          const rgf_options* opt, rgf_cplx* S, int64_t ldS,
+                                          rgf_channels* ch, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -85,6 +85,8 @@ SIGNATURES = {
     "rgf_last_profile": (c_int, [c_void_p, POINTER(c_int64), POINTER(c_double), POINTER(c_double), c_char_p,
                                  ctypes.c_size_t]),
     "rgf_set_stream": (c_int, [c_void_p, c_void_p]),
+    "rgf_smatrix_2d_noalloc": (c_int, [POINTER(Syst2D), POINTER(Request), POINTER(Options), c_void_p, c_int64,
+                                       POINTER(Channels), c_void_p]),
 }
 
 _lib = None

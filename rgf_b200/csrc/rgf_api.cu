@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <string>
 #include <chrono>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -29,9 +30,17 @@ namespace rgf {
 static thread_local std::string tl_err;
 void set_error(const std::string& msg) { tl_err = msg; }
 
+// Bump region of caller-independent device memory (the static scratch of
+// rgf_smatrix_2d_noalloc); buffers carved from it are never freed.
+struct Arena {
+  unsigned char* base = nullptr;
+  size_t cap = 0, used = 0;
+};
+
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  Arena* arena = nullptr;  // non-null: grow inside this arena instead of cudaMalloc
 };
 
 }  // namespace rgf
@@ -70,6 +79,18 @@ namespace {
 rgf_status ensure(DevBuf& b, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (b.bytes >= bytes) return RGF_OK;
+  if (b.arena) {
+    const size_t need = (bytes + 255) & ~(size_t)255;
+    if (b.arena->used + need > b.arena->cap) {
+      set_error("problem too large for the static device scratch of rgf_smatrix_2d_noalloc (" +
+                std::to_string(b.arena->cap >> 20) + " MiB): its workspace needs more; use rgf_smatrix_2d");
+      return RGF_ERR_ARG;
+    }
+    b.p = b.arena->base + b.arena->used;
+    b.bytes = bytes;
+    b.arena->used += need;
+    return RGF_OK;
+  }
   if (b.p) cudaFree(b.p);
   b.p = nullptr;
   b.bytes = 0;
@@ -772,6 +793,43 @@ rgf_status check_handle(rgf_handle h) {
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// static device scratch of rgf_smatrix_2d_noalloc
+// ---------------------------------------------------------------------------
+// Every GPU that loads this library holds this array until the process
+// exits.  In host code the name only stands for the device symbol; its device
+// address comes from cudaGetSymbolAddress, once per device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[RGF_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kMaxNoallocDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_ptr[kMaxNoallocDevices] = {};
+
+// address of the scratch array on the current device (resolved on the first
+// call on that device, with that device current)
+rgf_status noalloc_scratch(int device, unsigned char** out) {
+  if (device < 0 || device >= kMaxNoallocDevices) {
+    set_error("rgf_smatrix_2d_noalloc: device ordinal out of range");
+    return RGF_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      cudaGetLastError();
+      set_error(std::string("rgf_smatrix_2d_noalloc: cudaGetSymbolAddress of the static scratch failed: ") +
+                cudaGetErrorString(e));
+      return RGF_ERR_CUDA;
+    }
+    g_noalloc_ptr[device] = static_cast<unsigned char*>(p);
+  }
+  *out = g_noalloc_ptr[device];
+  return RGF_OK;
+}
+}  // namespace
+
 extern "C" {
 
 rgf_status rgf_create(int device, rgf_handle* out) {
@@ -965,6 +1023,39 @@ rgf_status rgf_last_stats(rgf_handle h, int64_t* kernel_launches, double* probe_
   if (kernel_launches) *kernel_launches = h->launches;
   if (probe_residual) *probe_residual = h->probe;
   return RGF_OK;
+}
+
+rgf_status rgf_smatrix_2d_noalloc(const rgf_syst2d* syst, const rgf_request* req, const rgf_options* opt,
+                                  rgf_cplx* S, int64_t ldS, rgf_channels* ch, void* stream) {
+  if (!syst) {
+    set_error("syst must be a structure");
+    return RGF_ERR_ARG;
+  }
+  if (opt && opt->profile > 0) {
+    set_error("rgf_smatrix_2d_noalloc: profiling is not available (it creates CUDA events)");
+    return RGF_ERR_ARG;
+  }
+  int device = 0;
+  RGF_CUDA_TRY(cudaGetDevice(&device));
+  unsigned char* base = nullptr;
+  rgf_status st;
+  if ((st = noalloc_scratch(device, &base))) return st;
+  // a handle on the stack whose every workspace buffer grows inside the
+  // static scratch; nothing in it owns device memory, so it is not destroyed
+  Arena arena;
+  arena.base = base;
+  arena.cap = RGF_NOALLOC_SCRATCH_BYTES;
+  rgf_handle_s h;
+  h.device = device;
+  h.stream = reinterpret_cast<cudaStream_t>(stream);
+  RGF_CUDA_TRY(cudaDeviceGetAttribute(&h.sms, cudaDevAttrMultiProcessorCount, device));
+  DevBuf* bufs[] = {&h.k0,      &h.k1,      &h.kx[0],     &h.kx[1],     &h.lam[0],  &h.lam[1],  &h.mu[0],
+                    &h.mu[1],   &h.isprop[0], &h.isprop[1], &h.prop[0], &h.prop[1], &h.conj[0], &h.conj[1],
+                    &h.nprop,   &h.status,  &h.phi,       &h.tmp,       &h.g0s,     &h.g0e,     &h.st_col,
+                    &h.st_val,  &h.eps,     &h.aug,       &h.pc,        &h.u,       &h.idx,     &h.sdev,
+                    &h.xpc,     &h.xrow,    &h.xt,        &h.xu,        &h.xsync,   &h.xprobe,  &h.xtrace};
+  for (DevBuf* b : bufs) b->arena = &arena;
+  return smatrix(&h, problem2d(syst), req, opt, S, ldS, ch);
 }
 
 }  // extern "C"
