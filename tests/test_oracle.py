@@ -196,3 +196,45 @@ def test_golden_small_fixtures_reproduce(path):
     fn = cal_smatrix_RGF if case["dim"] == "2d" else cal_smatrix_RGF_3D
     S, _ = fn(case["syst"], case["out"], case["in"])
     assert rel(S, case["S"]) < 1e-13
+
+
+# ---------------------------------------------------------------------------
+# permittivity gradient (an addition of this build; the reference has none)
+# ---------------------------------------------------------------------------
+GRAD_CASES = [
+    ("periodic", ["left", "right"], ["left", "right"]),
+    ("Dirichlet", {"ind_out_R": [1, 2]}, {"ind_in_L": [2, 1]}),
+    ("Neumann", ["left"], ["left"]),
+    (0.4, ["right"], ["left", "right"]),
+    ("DirichletNeumann", ["left", "right"], ["right"]),
+    ("periodic", {"ind_out_L": [1], "ind_out_R": [2, 1]}, {"ind_in_R": [1]}),
+]
+
+
+@pytest.mark.parametrize("bc,out,inp", GRAD_CASES)
+def test_adjoint_recursion_matches_dense_gradient(bc, out, inp):
+    """The backward recursions over the start-connected blocks give the same
+    dS/d eps as the dense inverse, for every request form and direction."""
+    from oracle.adjoint import grad_dense_2d, grad_rgf_2d
+    rng = np.random.default_rng(11)
+    syst = dict(epsilon=1 + 2 * rng.random((7, 5)) + 0.01j * rng.random((7, 5)), epsilon_L=1.0,
+                epsilon_R=1.3, k0dx=1.1, yBC=bc)
+    S0, _ = cal_smatrix_RGF(syst, out, inp)
+    D = rng.standard_normal(S0.shape) + 1j * rng.standard_normal(S0.shape)
+    _, g1 = grad_dense_2d(syst, out, inp, D)
+    _, g2 = grad_rgf_2d(syst, out, inp, D)
+    assert np.abs(g1 - g2).max() <= 1e-12 * np.abs(g1).max()
+
+
+@pytest.mark.parametrize("bc,out,inp", GRAD_CASES[:3])
+def test_adjoint_matches_finite_differences(bc, out, inp):
+    from oracle.adjoint import grad_fd_2d, grad_rgf_2d
+    rng = np.random.default_rng(12)
+    syst = dict(epsilon=1 + 2 * rng.random((7, 5)), epsilon_L=1.0, epsilon_R=1.0, k0dx=1.1, yBC=bc)
+    S0, _ = cal_smatrix_RGF(syst, out, inp)
+    D = rng.standard_normal(S0.shape) + 1j * rng.standard_normal(S0.shape)
+    _, g = grad_rgf_2d(syst, out, inp, D)
+    pix = [(1, 2), (6, 0), (3, 4)]
+    fd = grad_fd_2d(syst, out, inp, D, pix)
+    an = 2 * np.real(np.array([g[m, n] for m, n in pix]))
+    assert np.abs(an - fd).max() <= 1e-7 * np.abs(fd).max()
