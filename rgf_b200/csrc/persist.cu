@@ -15,9 +15,8 @@
 //    them in shared memory with TMA bulk copies (cp.async.bulk + mbarrier) and
 //    update the register tile with mma.sync.m8n8k4.f64.  The subtiles holding
 //    pieces of later steps go first and are published right away: the pivot
-//    rows W(J_{s+1}, Cq) and columns W(I, J_{s+1}) of step s+1, and three
-//    32x32 blocks of W after step s -- (J_{s+2},J_{s+2}), (J_{s+2},J_{s+1}),
-//    (J_{s+1},J_{s+2}) -- for the T-server.
+//    rows W(J_{s+1}, Cq) and columns W(I, J_{s+1}) of step s+1, and the
+//    32x32 block (J_{s+2},J_{s+2}) of W after step s for the T-server.
 //  * tile CTA, 1 panel warpgroup: its ceil(BN/TR)-column slice of U_s(Cq),
 //    on the FP64 tensor cores.
 //  * T-server CTA (one extra CTA on an SM of its own, so its FP64 pipe is not
@@ -209,7 +208,7 @@ struct Sync {
     u_flag = t_flag + 1;
     d_flag = u_flag + p.TR * p.TC;
     srv_flag = d_flag + 1;
-    d_used = srv_flag + 6;
+    d_used = srv_flag + 2;
     pc_cons = p.cons;
     row_cons = pc_cons + 2 * p.TR;
     t_cons = row_cons + 2 * p.TC;
@@ -307,60 +306,37 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
   const int S = p.L * p.NB;
   const int tr0 = I * BM, tc0 = Cq * BN;  // tile origin
 
-  // Urgent subtiles of this warp for the pieces published while step s runs:
-  // rows / columns of the window of step s1 = s+1 (rowU/colU) and, when s2 =
-  // s1+1 is in the same slice, the block (J_s2, J_s2) (rowU2 && colU2); the
-  // server blocks (J_s2,J_s1) and (J_s1,J_s2) lie inside colU / rowU.
-  // (bit mi / ni of the masks below)
-  unsigned rowU = 0, colU = 0, rowU2 = 0, colU2 = 0;
-  bool any_r = false, any_c = false, any_srv = false, any_urg = false;
-  auto set_urgency = [&](int s1, bool with_srv) {
-    const int w1 = (s1 % p.NB) * kPB, w2 = w1 + kPB;
-    rowU = colU = rowU2 = colU2 = 0;
-#pragma unroll
-    for (int mi = 0; mi < MI; mi++) {
-      const int r0 = t.r_base + mi * 8;
-      rowU |= (unsigned)(r0 >= w1 && r0 < w1 + kPB) << mi;
-      rowU2 |= (unsigned)(with_srv && r0 >= w2 && r0 < w2 + kPB) << mi;
-    }
-#pragma unroll
-    for (int ni = 0; ni < NI; ni++) {
-      const int c0 = t.c_base + ni * 8;
-      colU |= (unsigned)(c0 >= w1 && c0 < w1 + kPB) << ni;
-      colU2 |= (unsigned)(with_srv && c0 >= w2 && c0 < w2 + kPB) << ni;
-    }
-    any_r = rowU != 0;
-    any_c = colU != 0;
-    any_srv = (rowU2 && colU2) || (rowU2 && colU) || (rowU && colU2);
-    any_urg = any_r || any_c || (rowU2 && colU2);
-  };
-  auto clear_urgency = [&]() {
-    any_r = any_c = any_srv = any_urg = false;
-    rowU = colU = rowU2 = colU2 = 0;
-  };
-  auto bit = [](unsigned m, int i) { return ((m >> i) & 1u) != 0; };
-  // The warps of this CTA that publish a kind of piece for step s1, and the
-  // lowest of them (the one that releases the flags), computed on demand so
-  // that nothing of it stays live across the update passes.
+  // Publication sets.  After the update of step s the warps holding pieces
+  // of step s1 = s+1 publish them: the pivot rows / columns of s1 (glob), at
+  // a slice start the first pivot block (djj), and, when s2 = s1+1 is in the
+  // same slice, three 32x32 blocks of W for the T-server (srv).  Membership
+  // depends only on the warp's row / column range, so every warp evaluates
+  // it for every warp of the CTA (barrier counts, flag-releasing lead).
   enum { kSetGlob, kSetDjj, kSetSrv };
-  auto pub_set = [&](int kind, int s1, int* lead) {
+  auto in_set = [&](int kind, int w, int s1) {
     const int w1 = (s1 % p.NB) * kPB, w2 = w1 + kPB;
+    const int rb = tr0 + (w >> 2) * Tile::WR, cb = tc0 + (w & 3) * Tile::WC;
+    const bool r1 = (w1 + kPB > rb) && (w1 < rb + Tile::WR);
+    const bool c1 = (w1 + kPB > cb) && (w1 < cb + Tile::WC);
+    const bool r2 = (w2 + kPB > rb) && (w2 < rb + Tile::WR);
+    const bool c2 = (w2 + kPB > cb) && (w2 < cb + Tile::WC);
+    return kind == kSetGlob ? (r1 || c1) : kind == kSetDjj ? (r1 && c1) : (r2 && c2);
+  };
+  auto pub_set = [&](int kind, int s1, int* lead) {
     int n = 0;
     *lead = -1;
-    for (int w = kMathWarps - 1; w >= 0; w--) {
-      const int rb = tr0 + (w >> 2) * Tile::WR, cb = tc0 + (w & 3) * Tile::WC;
-      const bool r1 = (w1 + kPB > rb) && (w1 < rb + Tile::WR);
-      const bool c1 = (w1 + kPB > cb) && (w1 < cb + Tile::WC);
-      const bool r2 = (w2 + kPB > rb) && (w2 < rb + Tile::WR);
-      const bool c2 = (w2 + kPB > cb) && (w2 < cb + Tile::WC);
-      const bool in = kind == kSetGlob ? (r1 || c1) : kind == kSetDjj ? (r1 && c1) : ((r2 && c2) || (r2 && c1) || (r1 && c2));
-      if (in) {
+    for (int w = kMathWarps - 1; w >= 0; w--)
+      if (in_set(kind, w, s1)) {
         n++;
         *lead = w;
       }
-    }
     return n;
   };
+  // does subtile row mi / column ni of this warp lie in the 32-wide window at w
+  auto row_in = [&](int mi, int w) { return (unsigned)(t.r_base + mi * 8 - w) < (unsigned)kPB; };
+  auto col_in = [&](int ni, int w) { return (unsigned)(t.c_base + ni * 8 - w) < (unsigned)kPB; };
+  const int lr = t.lane >> 2, lc = (t.lane & 3) * 2;  // this thread's row / column within a subtile
+  const int sw = (lr & 1) << 2;                       // swzA swizzle of this thread's rows
   auto load_tile = [&]() {
 #pragma unroll
     for (int mi = 0; mi < MI; mi++)
@@ -385,62 +361,66 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
           if (i < p.R && j < p.C) __stcg(p.M + (int64_t)i * p.ldm + j, cmk(t.acc[mi][ni][h], t.acc[mi][ni][2 + h]));
         }
   };
-  // rank-32 update of a subset of this warp's subtiles: 0 all, 1 urgent, 2 the rest.
-  // First halves of every complex product, then the dependent second halves.
-  auto mma_pass = [&](const int mode) {
-    auto sel = [&](int mi, int ni) {
-      const bool u = bit(rowU, mi) || bit(colU, ni) || (bit(rowU2, mi) && bit(colU2, ni));
-      return (mode == 0) || (mode == 1 && u) || (mode == 2 && !u);
-    };
+  // rank-32 update of the whole warp tile: first halves of every complex
+  // product, then the dependent second halves
+  auto mma_pass = [&]() {
 #pragma unroll
     for (int kk = 0; kk < kPB / 4; kk++) {
       double2 b[NI];
 #pragma unroll
       for (int ni = 0; ni < NI; ni++)
-        b[ni] = sh.op.B[swzB<BN>(kk * 4 + (t.lane & 3), t.wc * Tile::WC + ni * 8 + (t.lane >> 2))];
+        b[ni] = sh.op.B[swzB<BN>(kk * 4 + (t.lane & 3), t.wc * Tile::WC + ni * 8 + lr)];
 #pragma unroll
       for (int mi = 0; mi < MI; mi++) {
-        const double ax = sh.op.A[swzA(t.wr * Tile::WR + mi * 8 + (t.lane >> 2), kk * 4 + (t.lane & 3))].x;
+        const double ax = sh.op.A[swzA(t.wr * Tile::WR + mi * 8 + lr, kk * 4 + (t.lane & 3))].x;
 #pragma unroll
-        for (int ni = 0; ni < NI; ni++)
-          if (sel(mi, ni)) {
-            dmma(t.acc[mi][ni][0], t.acc[mi][ni][1], ax, b[ni].x);
-            dmma(t.acc[mi][ni][2], t.acc[mi][ni][3], ax, b[ni].y);
-          }
+        for (int ni = 0; ni < NI; ni++) {
+          dmma(t.acc[mi][ni][0], t.acc[mi][ni][1], ax, b[ni].x);
+          dmma(t.acc[mi][ni][2], t.acc[mi][ni][3], ax, b[ni].y);
+        }
       }
 #pragma unroll
       for (int mi = 0; mi < MI; mi++) {
-        const double ay = sh.op.A[swzA(t.wr * Tile::WR + mi * 8 + (t.lane >> 2), kk * 4 + (t.lane & 3))].y;
+        const double ay = sh.op.A[swzA(t.wr * Tile::WR + mi * 8 + lr, kk * 4 + (t.lane & 3))].y;
 #pragma unroll
-        for (int ni = 0; ni < NI; ni++)
-          if (sel(mi, ni)) {
-            dmma(t.acc[mi][ni][0], t.acc[mi][ni][1], -ay, b[ni].y);
-            dmma(t.acc[mi][ni][2], t.acc[mi][ni][3], ay, b[ni].x);
-          }
+        for (int ni = 0; ni < NI; ni++) {
+          dmma(t.acc[mi][ni][0], t.acc[mi][ni][1], -ay, b[ni].y);
+          dmma(t.acc[mi][ni][2], t.acc[mi][ni][3], ay, b[ni].x);
+        }
       }
     }
   };
-  // the first pivot block of a slice -> djjbuf for the T-server (all its warps call it)
+  // 32x32 block (rows in window wr_, columns in window wc_) of W into a
+  // row-major [32][32] buffer; rows / columns at or beyond `lim` are padded
+  // with the identity (pad_id) or zeros
+  auto store_block = [&](double2* dst, int wr_, int wc_, int lim_r, int lim_c, bool pad_id) {
+#pragma unroll
+    for (int mi = 0; mi < MI; mi++) {
+      if (!row_in(mi, wr_)) continue;
+      const int r = t.r_base + mi * 8 + lr - wr_;
+#pragma unroll
+      for (int ni = 0; ni < NI; ni++) {
+        if (!col_in(ni, wc_)) continue;
+        const int c0 = t.c_base + ni * 8 + lc - wc_;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int c = c0 + h;
+          const bool in = r < lim_r && c < lim_c;
+          const double2 v = in ? cmk(t.acc[mi][ni][h], t.acc[mi][ni][2 + h])
+                               : cmk((pad_id && r == c) ? 1.0 : 0.0, 0.0);
+          __stcg(dst + r * kPB + c, v);
+        }
+      }
+    }
+  };
+  // the first pivot block of a slice -> djjbuf for the T-server
   auto publish_djj = [&](int s1) {
     const int w0 = (s1 % p.NB) * kPB;
     const int jnn = min(kPB, p.N - w0);
     int ok = 1;
     if (t.lane == 0 && s1 >= p.NB) ok = wait_ge(p, sy.d_used, s1 - p.NB);  // previous slice's was loaded
     ok = __shfl_sync(kFull, ok, 0);
-    if (ok) {
-#pragma unroll
-      for (int mi = 0; mi < MI; mi++)
-#pragma unroll
-        for (int ni = 0; ni < NI; ni++)
-#pragma unroll
-          for (int h = 0; h < 2; h++) {
-            if (!(bit(rowU, mi) && bit(colU, ni))) continue;
-            const int r = t.row(mi) - w0, c = t.col(ni, h) - w0;
-            const double2 v = (r < jnn && c < jnn) ? cmk(t.acc[mi][ni][h], t.acc[mi][ni][2 + h])
-                                                   : cmk(r == c ? 1.0 : 0.0, 0.0);
-            __stcg(p.djjbuf + r * kPB + c, v);
-          }
-    }
+    if (ok) store_block(p.djjbuf, w0, w0, jnn, jnn, true);
     int lead;
     const int n = pub_set(kSetDjj, s1, &lead);
     const int all_ok = !bar_or(kBarDjj, n * 32, !ok);
@@ -458,6 +438,8 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
     int lead;
     const int n = pub_set(kSetGlob, s1, &lead);
     if (warp == lead && t.lane == 0) trace_ev(p, s1 - 1, kTrGlobEnter);
+    const bool any_r = t.r_base + Tile::WR > w0 && t.r_base < w0 + kPB;
+    const bool any_c = t.c_base + Tile::WC > w0 && t.c_base < w0 + kPB;
     int ok = 1;
     if (t.lane == 0 && s1 >= 2) {
       if (any_r) ok &= wait_ge(p, sy.row_cons + par * p.TC + Cq, p.TR * (s1 >> 1));
@@ -465,29 +447,41 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
     }
     ok = __shfl_sync(kFull, ok, 0);
     if (ok) {
-      double2* rowb = p.rowbuf + ((size_t)par * p.TC + Cq) * (kPB * BN);
-      double2* pcb = p.pcbuf + ((size_t)par * p.TR + I) * (BM * kPB);
+      // pivot rows: rowbuf[k][c - tc0], zero beyond the last pivot row
+      double2* rowb = p.rowbuf + ((size_t)par * p.TC + Cq) * (kPB * BN) + (t.c_base - tc0 + lc);
 #pragma unroll
-      for (int mi = 0; mi < MI; mi++)
+      for (int mi = 0; mi < MI; mi++) {
+        if (!row_in(mi, w0)) continue;
+        const int kr = t.r_base + mi * 8 + lr - w0;
+        const bool valid = kr < jnn;
+        double2* q = rowb + kr * BN;
 #pragma unroll
         for (int ni = 0; ni < NI; ni++)
 #pragma unroll
+          for (int h = 0; h < 2; h++)
+            __stcg(q + ni * 8 + h, valid ? cmk(t.acc[mi][ni][h], t.acc[mi][ni][2 + h]) : cmk(0.0, 0.0));
+      }
+      // pivot columns: Pc = [-W(i, J) ; +I on the pivot rows], zero beyond the
+      // last pivot column and below row R, stored in the swizzled [BM][32] layout
+      double2* pcb = p.pcbuf + ((size_t)par * p.TR + I) * (BM * kPB) + (t.r_base - tr0 + lr) * kPB;
+#pragma unroll
+      for (int ni = 0; ni < NI; ni++) {
+        if (!col_in(ni, w0)) continue;
+        const int kc = t.c_base + ni * 8 - w0;  // multiple of 8: the swizzle acts on lc + h only
+#pragma unroll
+        for (int mi = 0; mi < MI; mi++) {
+          const int i = t.r_base + mi * 8 + lr;
+#pragma unroll
           for (int h = 0; h < 2; h++) {
-            const int i = t.row(mi), j = t.col(ni, h);
-            const double2 v = cmk(t.acc[mi][ni][h], t.acc[mi][ni][2 + h]);
-            if (bit(rowU, mi)) {
-              const int k = (int)(i - w0);
-              __stcg(rowb + k * BN + (int)(j - tc0), (k < jnn) ? v : cmk(0.0, 0.0));
-            }
-            if (bit(colU, ni)) {
-              const int k = (int)(j - w0);
-              double2 wv;
-              if (k >= jnn || i >= p.R) wv = cmk(0.0, 0.0);
-              else if (i >= w0 && i < w0 + jnn) wv = cmk((i - w0 == k) ? 1.0 : 0.0, 0.0);
-              else wv = cneg(v);
-              __stcg(pcb + swzA((int)(i - tr0), k), wv);
-            }
+            const int k = kc + lc + h;
+            double2 wv;
+            if (k >= jnn || i >= p.R) wv = cmk(0.0, 0.0);
+            else if (i >= w0 && i < w0 + jnn) wv = cmk((i - w0 == k) ? 1.0 : 0.0, 0.0);
+            else wv = cmk(-t.acc[mi][ni][h], -t.acc[mi][ni][2 + h]);
+            __stcg(pcb + mi * 8 * kPB + kc + ((lc + h) ^ sw), wv);
           }
+        }
+      }
     }
     if (warp == lead && t.lane == 0) trace_ev(p, s1 - 1, kTrGlobStored);
     const int all_ok = !bar_or(kBarPub, n * 32, !ok);
@@ -498,9 +492,8 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
       trace_ev(p, s1 - 1, kTrMathPublished);
     }
   };
-  // blocks (J_s2,J_s2), (J_s2,J_s1), (J_s1,J_s2) of the current W, s2 = s1+1,
-  // for the T-server's Schur update of step s2.  Beyond the last pivot row
-  // the first block is padded with the identity and the others with zeros.
+  // block (J_s2, J_s2) of the current W, s2 = s1+1, for the T-server's Schur
+  // update of step s2 (padded with the identity beyond the last pivot row)
   auto publish_srv = [&](int s1) {
     const int s2 = s1 + 1;
     const int w1 = (s1 % p.NB) * kPB, w2 = w1 + kPB;
@@ -513,49 +506,28 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
     if (t.lane == 0 && s2 >= 2) ok = wait_ge(p, sy.srv_cons + par, s2 >> 1);
     ok = __shfl_sync(kFull, ok, 0);
     if (ok) {
-      double2* sb = p.srvbuf + (size_t)par * 3 * kPB * kPB;
-#pragma unroll
-      for (int mi = 0; mi < MI; mi++)
-#pragma unroll
-        for (int ni = 0; ni < NI; ni++)
-#pragma unroll
-          for (int h = 0; h < 2; h++) {
-            const int i = t.row(mi), j = t.col(ni, h);
-            const double2 v = cmk(t.acc[mi][ni][h], t.acc[mi][ni][2 + h]);
-            const int r2 = (int)(i - w2), c2 = (int)(j - w2), r1 = (int)(i - w1), c1 = (int)(j - w1);
-            if (bit(rowU2, mi) && bit(colU2, ni))
-              __stcg(sb + r2 * kPB + c2, (r2 < jn2 && c2 < jn2) ? v : cmk(r2 == c2 ? 1.0 : 0.0, 0.0));
-            if (bit(rowU2, mi) && bit(colU, ni)) __stcg(sb + kPB * kPB + r2 * kPB + c1, (r2 < jn2) ? v : cmk(0.0, 0.0));
-            if (bit(rowU, mi) && bit(colU2, ni)) __stcg(sb + 2 * kPB * kPB + r1 * kPB + c2, (c2 < jn2) ? v : cmk(0.0, 0.0));
-          }
+      store_block(p.srvbuf + (size_t)par * kPB * kPB, w2, w2, jn2, jn2, true);
     }
     if (warp == lead && t.lane == 0) trace_ev(p, s1 - 1, kTrSrvPubStored);
     const int all_ok = !bar_or(kBarSrv, n * 32, !ok);
     if (warp == lead && t.lane == 0 && all_ok) {
       __threadfence();
-      const bool rin1 = w1 >= tr0 && w1 < tr0 + BM, rin2 = w2 >= tr0 && w2 < tr0 + BM;
-      const bool cin1 = w1 >= tc0 && w1 < tc0 + BN, cin2 = w2 >= tc0 && w2 < tc0 + BN;
-      int* f = sy.srv_flag + par * 3;
-      if (rin2 && cin2) st_release(f + 0, s2);
-      if (rin2 && cin1) st_release(f + 1, s2);
-      if (rin1 && cin2) st_release(f + 2, s2);
+      st_release(sy.srv_flag + par, s2);
       trace_ev(p, s1 - 1, kTrSrvPubDone);
     }
   };
-  // every piece this warp holds at the start of a slice (kernel start, or
-  // after the slice assembly): the first pivot block for the T-server, the
-  // first pivot rows / columns, and the server blocks of the second step
-  auto publish_start = [&](int s1) {
-    const bool with_srv = p.NB >= 2;
-    set_urgency(s1, with_srv);
-    if (any_r && any_c) publish_djj(s1);
-    if (any_r || any_c) publish_glob(s1);
-    if (any_srv) publish_srv(s1);
+  // every piece of step s1 this warp holds; at a slice start (kernel start or
+  // after the slice assembly) also the first pivot block
+  auto publish = [&](int s1, bool slice_start) {
+    const bool with_srv = (s1 % p.NB) + 1 <= p.NB - 1;  // step s1 + 1 is in the same slice
+    if (slice_start && in_set(kSetDjj, warp, s1)) publish_djj(s1);
+    if (in_set(kSetGlob, warp, s1)) publish_glob(s1);
+    if (with_srv && in_set(kSetSrv, warp, s1)) publish_srv(s1);
   };
 
   load_tile();
   bar_sync(kBarMath, kMathThreads);
-  publish_start(0);
+  publish(0, true);
 
   double probe_max = 0.0;
   for (int s = 0; s < S; s++) {
@@ -639,29 +611,17 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           const int i = t.row(mi), j = t.col(ni, h);
-          if ((i >= j0 && i < j0 + jn) || (j >= j0 && j < j0 + jn)) {
+          if ((unsigned)(i - j0) < (unsigned)jn || (unsigned)(j - j0) < (unsigned)jn) {
             t.acc[mi][ni][h] = 0.0;
             t.acc[mi][ni][2 + h] = 0.0;
           }
         }
-    // ---- rank-32 update; pieces of later steps first ----
+    // ---- rank-32 update, then the pieces of step s+1 ----
     const int s1 = s + 1;
     const bool last_block = (k == p.NB - 1);
     const bool slice_end = last_block && (s1 < S);
-    if (last_block) {
-      clear_urgency();
-    } else {
-      const bool with_srv = (k + 2 <= p.NB - 1);  // step s1 + 1 is in this slice
-      set_urgency(s1, with_srv);
-    }
-    if (!any_urg) {
-      mma_pass(0);
-    } else {
-      mma_pass(1);
-      if (any_r || any_c) publish_glob(s1);
-      if (any_srv) publish_srv(s1);
-      mma_pass(2);
-    }
+    mma_pass();
+    if (!last_block) publish(s1, false);
     if (tid == 0) trace_ev(p, s, kTrMathDone);
     if (last_block) {
       // slice boundary: the tile goes to its home in W, the probe is checked
@@ -675,7 +635,7 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
       bar_sync(kBarMath, kMathThreads);
       if (slice_end) {
         load_tile();
-        publish_start(s1);
+        publish(s1, true);
       }
     }
   }
@@ -863,7 +823,13 @@ __device__ __forceinline__ void blk_gemm(const Blk& A, const Blk& B, const Blk* 
 }
 
 // the 8 math warps of the server CTA form and invert every pivot block one
-// step ahead of the bulk update
+// step ahead of the bulk update.  For step s (not the first of its slice):
+//   a1 = W^{(s-2)}(J_s, J_s)      from srvbuf (published after step s-2)
+//   a2 = W^{(s-2)}(J_s, J_{s-1})  = -(pivot columns of step s-1, rows J_s)
+//   a3 = W^{(s-2)}(J_{s-1}, J_s)  =   pivot rows of step s-1, columns J_s
+// The pivot buffers of step s-1 stay valid until they are published for
+// step s+1, which needs T_s from this CTA.
+template <int BM, int BN>
 __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, int t) {
   const int lane = t & 31, warp = t >> 5;
   const int S = p.L * p.NB;
@@ -878,8 +844,9 @@ __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, 
       if (k == 0) {
         ok = wait_ge(p, sy.d_flag, s);
       } else {
-        const int* f = sy.srv_flag + par * 3;
-        ok = wait_ge(p, f + 0, s) && wait_ge(p, f + 1, s) && wait_ge(p, f + 2, s);
+        const int w = k * kPB;
+        ok = wait_ge(p, sy.srv_flag + par, s) && wait_ge(p, sy.pc_flag + w / BM, s - 1) &&
+             wait_ge(p, sy.row_flag + w / BN, s - 1);
       }
       sh.panel_abort = !ok;
       trace_ev(p, s, kTrPanelTin);
@@ -889,11 +856,18 @@ __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, 
     if (k == 0) {
       for (int e = t; e < kPB * kPB; e += kServerThreads) sh.srv.a1[e / kPB][e % kPB] = __ldcg(p.djjbuf + e);
     } else {
-      const double2* sb = p.srvbuf + (size_t)par * 3 * kPB * kPB;
+      const double2* sb = p.srvbuf + (size_t)par * kPB * kPB;
+      const int w = k * kPB, parq = par ^ 1;
+      const int I2 = w / BM, C2 = w / BN;
+      const double2* pcb = p.pcbuf + ((size_t)parq * p.TR + I2) * (BM * kPB) + (size_t)(w - I2 * BM) * kPB;
+      const double2* rwb = p.rowbuf + ((size_t)parq * p.TC + C2) * (kPB * BN) + (w - C2 * BN);
       for (int e = t; e < kPB * kPB; e += kServerThreads) {
-        sh.srv.a1[e / kPB][e % kPB] = __ldcg(sb + e);
-        sh.srv.a2[e / kPB][e % kPB] = __ldcg(sb + kPB * kPB + e);
-        sh.srv.a3[e / kPB][e % kPB] = __ldcg(sb + 2 * kPB * kPB + e);
+        const int r = e / kPB, c = e % kPB;
+        sh.srv.a1[r][c] = __ldcg(sb + e);
+        const double2 pcv = __ldcg(pcb + r * kPB + (c ^ ((r & 1) << 2)));
+        sh.srv.a2[r][c] = r < jn ? cneg(pcv) : cmk(0.0, 0.0);
+        const double2 rwv = __ldcg(rwb + r * BN + c);
+        sh.srv.a3[r][c] = c < jn ? rwv : cmk(0.0, 0.0);
       }
     }
     if (t < kPB) sh.perm[t] = t;
@@ -953,7 +927,7 @@ __global__ void __launch_bounds__(Cfg<BM, BN>::Threads, 1) k_persist(PersistPara
   static_assert(Cfg<BM, BN>::MathThreads == kServerThreads, "the server uses the math warpgroups");
   if (threadIdx.x < Cfg<BM, BN>::MathThreads) {
     asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(Cfg<BM, BN>::MathRegs));
-    if (server) server_role(p, sh, sy, threadIdx.x);
+    if (server) server_role<BM, BN>(p, sh, sy, threadIdx.x);
     else math_role<BM, BN>(p, sh, sy, I, Cq);
   } else {
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(Cfg<BM, BN>::PanelRegs));

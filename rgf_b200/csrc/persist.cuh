@@ -22,8 +22,8 @@ struct PersistParams {
   double2* tbuf;         // [2][32][32]
   double2* ubuf;         // [2][TC][32][BN]
   double2* djjbuf;       // [32][32] first pivot block of a slice, for the T-server CTA
-  double2* srvbuf;       // [2][3][32][32] blocks the T-server updates into the next pivot block
-  int* flags;            // pc[TR], row[TC], t[1], u[TC*TR], d[1], srv[2][3], d_used[1]  (init -1)
+  double2* srvbuf;       // [2][32][32] block the T-server updates into the next pivot block
+  int* flags;            // pc[TR], row[TC], t[1], u[TC*TR], d[1], srv[2], d_used[1]  (init -1)
   int* cons;             // pc[2][TR], row[2][TC], t[2], u[2][TC], srv[2]             (init 0)
   int* status;           // kStatus* bits
   int* abort;            // raised by the first wait that times out
@@ -44,7 +44,7 @@ enum { kTrMathStart = 0, kTrMathOperands, kTrMathCopied, kTrMathPublished, kTrMa
        // publication of the pivot rows / columns and of the server blocks (lead warp)
        kTrGlobEnter, kTrGlobStored, kTrSrvPubEnter, kTrSrvPubStored, kTrSrvPubDone, kTraceEvents };
 
-inline int persist_flag_words(int TR, int TC) { return TR + TC + 1 + TR * TC + 1 + 6 + 1; }
+inline int persist_flag_words(int TR, int TC) { return TR + TC + 1 + TR * TC + 1 + 2 + 1; }
 inline int persist_cons_words(int TR, int TC) { return 2 * TR + 2 * TC + 2 + 2 * TC + 2; }
 
 size_t persist_smem_bytes();

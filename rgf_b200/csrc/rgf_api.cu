@@ -555,7 +555,7 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
     const int nflags = persist_flag_words(TR, TC), ncons = persist_cons_words(TR, TC);
     if ((st = ensure(h->xpc, sizeof(double2) * 2 * TR * BMp * 32))) return st;
     if ((st = ensure(h->xrow, sizeof(double2) * 2 * TC * 32 * BNp))) return st;
-    if ((st = ensure(h->xt, sizeof(double2) * 9 * 32 * 32))) return st;  // tbuf[2], djjbuf, srvbuf[2][3]
+    if ((st = ensure(h->xt, sizeof(double2) * 5 * 32 * 32))) return st;  // tbuf[2], djjbuf, srvbuf[2]
     if ((st = ensure(h->xu, sizeof(double2) * 2 * TC * 32 * BNp))) return st;
     if ((st = ensure(h->xsync, sizeof(int) * (nflags + ncons + 4)))) return st;
     if ((st = ensure(h->xprobe, sizeof(unsigned long long)))) return st;
