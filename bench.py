@@ -203,6 +203,54 @@ def measure_fp64_peak(device: int):
     return FP64_DMMA_FALLBACK_TFLOPS, "fallback: earlier FP64 DMMA measurement on this pool (37 TFLOP/s)"
 
 
+def grad_over_fwd(h, dev, stream, reps: int = 3):
+    """Config-5 adjoint cost: time of rgf_smatrix_grad_2d (S and dF/d eps for
+    F = sum |t_ab|^2 over 8 left inputs -> 8 right outputs, checkpoint every 23
+    slices) over the time of the forward rgf_smatrix_2d, both device-resident
+    and timed with CUDA events on the library's stream."""
+    import torch
+
+    from rgf_b200 import _abi, workloads
+    syst, out, in_ = workloads.config5()
+    ny, nx = syst["epsilon"].shape
+    eps = torch.from_numpy(np.ascontiguousarray(syst["epsilon"].astype(complex).ravel(order="F"))).to(f"cuda:{dev}")
+    sy = _abi.Syst2D(ny, nx, eps.data_ptr(), 1, _abi.cplx(1.0), _abi.cplx(1.0), _abi.cplx(syst["k0dx"]),
+                     _abi.BC_PERIODIC, 0.0)
+    idx = np.arange(8, dtype=np.int64)
+    req = _abi.Request(None, 0, idx.ctypes.data, 8, idx.ctypes.data, 8, None, 0)
+    opt = _abi.Options(_abi.RGF_FP64, 0, 1, 0)
+    S = torch.zeros((8, 8), dtype=torch.complex128, device=f"cuda:{dev}")
+    g = torch.zeros((nx, ny), dtype=torch.complex128, device=f"cuda:{dev}")
+    lib = h.lib
+
+    def fwd():
+        _abi.check(lib.rgf_smatrix_2d(h.h, ctypes.byref(sy), ctypes.byref(req), ctypes.byref(opt), S.data_ptr(), 8,
+                                      None))
+
+    def grad():
+        D = S.conj().contiguous()
+        _abi.check(lib.rgf_smatrix_grad_2d(h.h, ctypes.byref(sy), ctypes.byref(req), ctypes.byref(opt),
+                                           D.data_ptr(), 8, S.data_ptr(), 8, g.data_ptr(), 23))
+
+    def t(fn):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    tf = t(fwd)
+    tg = t(grad)
+    return {"value": tg / tf, "fwd_ms": tf, "grad_ms": tg,
+            "workload": "config5: 2D periodic N=256, L=512, eps 1+3U, k0dx=2pi/15, t = S(out R 1:8, in L 1:8), "
+                        "F = sum|t|^2, checkpoint every 23 slices"}
+
+
 def config_dict():
     return {"workload": "config2: 2D Dirichlet, N=1024 transverse sites, L=4096 slices, eps 2.25 + 30% disks "
                         "(r 4-12 px) of 1 + 1j*U[0,0.01), k0dx=2pi/20, full S (P=102 per side, 204x204)",
@@ -303,7 +351,7 @@ def run_ours(args, dist):
     line["canonical_flops_per_S"] = F
     line["canonical_tflops"] = F * value / 1e12 / dist.world
     line["precision_form"] = None
-    line["grad_over_fwd"] = None
+    line["grad_over_fwd"] = grad_over_fwd(h, dev, stream) if not args.slices else None
     n, ms, fl_exec, name = prof
     fl = nx * workloads.canonical_slice_flops(ny, n_in // 2, n_out // 2)  # the launch covers all nx slices
     achieved = fl / (ms / n / 1e3) / 1e12 if n else None

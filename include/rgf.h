@@ -149,6 +149,25 @@ RGF_API rgf_status rgf_smatrix_2d(rgf_handle h, const rgf_syst2d* syst, const rg
 RGF_API rgf_status rgf_smatrix_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_request* req,
                           const rgf_options* opt, rgf_cplx* S, int64_t ldS, rgf_channels* ch);
 
+/* Permittivity gradient (an addition: the reference computes S only).
+ * Computes S as rgf_smatrix_2d/3d and
+ *     g[m + n*N] = sum_ab D[a + b*ldD] * dS_ab / d epsilon[m, n]
+ * for the caller's weights D (n_out x n_in, the row/column order of S), with
+ * m the transverse site (N = ny, or nx*ny in 3D, x fastest) and n the slice.
+ * For a real objective F of S with dF = 2 Re sum_ab D_ab dS_ab (e.g. D = conj(S)
+ * for F = sum |S_ab|^2), dF/d Re(eps) = 2 Re g and dF/d Im(eps) = -2 Im g.
+ * Method: the forward sweep keeps a checkpoint every `checkpoint` slices
+ * (<= 0: ceil(sqrt(L))); the backward pass recomputes one segment at a time
+ * and runs the recursions Psi_k = [X_k, 0] + g_k Psi_{k+1},
+ * Phi_k = [Z_k; 0] + Phi_{k+1} g_k over the start-connected slice inverses g_k.
+ * D, S and g are device pointers when opt->S_on_device, host otherwise. */
+RGF_API rgf_status rgf_smatrix_grad_2d(rgf_handle h, const rgf_syst2d* syst, const rgf_request* req,
+                                       const rgf_options* opt, const rgf_cplx* D, int64_t ldD, rgf_cplx* S,
+                                       int64_t ldS, rgf_cplx* g, int64_t checkpoint);
+RGF_API rgf_status rgf_smatrix_grad_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_request* req,
+                                       const rgf_options* opt, const rgf_cplx* D, int64_t ldD, rgf_cplx* S,
+                                       int64_t ldS, rgf_cplx* g, int64_t checkpoint);
+
 /* Size of the S block a request selects (needs the channel count, so it runs
  * the channel set-up on the device). */
 RGF_API rgf_status rgf_smatrix_size_2d(rgf_handle h, const rgf_syst2d* syst, const rgf_request* req,

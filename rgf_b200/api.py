@@ -282,6 +282,65 @@ def cal_smatrix_RGF_3D(syst, out, in_, *, device: int = 0, options=None, handle=
     return S, _channels_dict_3d(cb, nx, ny, bc)
 
 
+def smatrix_grad_RGF(syst, out, in_, D, *, checkpoint: int = 0, device: int = 0, options=None, handle=None):
+    """(S, g) for a 2D syst: S as cal_smatrix_RGF, and
+    g[m, n] = sum_ab D[a, b] dS_ab / d epsilon[m, n] (complex, shape [ny, nx]).
+
+    For a real objective F(S) with dF = 2 Re sum D dS (D = conj(S) for
+    F = sum |S|^2), dF/d Re(epsilon) = 2 Re g.  An addition of this library:
+    the reference computes S only."""
+    _check_syst(syst, "yBC")
+    eps = np.asarray(_get(syst, "epsilon"))
+    if eps.ndim != 2 or not np.issubdtype(eps.dtype, np.number):
+        raise ValueError("syst.epsilon must be a numeric matrix")
+    ny, nx = eps.shape
+    bc, ka = _bc_2d(_get(syst, "yBC"))
+    req, keep = _request(out, in_)
+    h = handle or _abi.default_handle(device)
+    epsf = np.ascontiguousarray(eps.astype(complex).ravel(order="F"))
+    sy = Syst2D(ny, nx, ptr(epsf), 0, cplx(_get(syst, "epsilon_L")), cplx(_get(syst, "epsilon_R")),
+                cplx(_get(syst, "k0dx")), bc, ka)
+    no, ni = ctypes.c_int64(), ctypes.c_int64()
+    check(h.lib.rgf_smatrix_size_2d(h.h, ctypes.byref(sy), ctypes.byref(req), ctypes.byref(no), ctypes.byref(ni)))
+    Dm = np.asfortranarray(np.asarray(D, dtype=complex).reshape(no.value, ni.value))
+    S = np.zeros((max(no.value, 1), max(ni.value, 1)), dtype=complex, order="F")
+    g = np.zeros((ny, nx), dtype=complex, order="F")
+    Dp = Dm if Dm.size else np.zeros((1, 1), dtype=complex, order="F")
+    opt = _options(options)
+    check(h.lib.rgf_smatrix_grad_2d(h.h, ctypes.byref(sy), ctypes.byref(req), ctypes.byref(opt), Dp.ctypes.data,
+                                    max(no.value, 1), S.ctypes.data, S.shape[0], g.ctypes.data, int(checkpoint)))
+    del keep
+    S = S[:no.value, :ni.value] if (no.value and ni.value) else np.zeros((no.value, ni.value))
+    return S, g
+
+
+def smatrix_grad_RGF_3D(syst, out, in_, D, *, checkpoint: int = 0, device: int = 0, options=None, handle=None):
+    """(S, g) for a 3D syst; g has the shape of syst.epsilon ([nx, ny, nz])."""
+    _check_syst(syst, "xyBC")
+    eps = np.asarray(_get(syst, "epsilon"))
+    if eps.ndim == 2:
+        eps = eps[:, :, None]
+    nx, ny, nz = eps.shape
+    bc, kxa, kya = _bc_3d(_get(syst, "xyBC"))
+    req, keep = _request(out, in_)
+    h = handle or _abi.default_handle(device)
+    epsf = np.ascontiguousarray(eps.astype(complex).ravel(order="F"))
+    sy = Syst3D(nx, ny, nz, ptr(epsf), 0, cplx(_get(syst, "epsilon_L")), cplx(_get(syst, "epsilon_R")),
+                cplx(_get(syst, "k0dx")), bc, kxa, kya)
+    no, ni = ctypes.c_int64(), ctypes.c_int64()
+    check(h.lib.rgf_smatrix_size_3d(h.h, ctypes.byref(sy), ctypes.byref(req), ctypes.byref(no), ctypes.byref(ni)))
+    Dm = np.asfortranarray(np.asarray(D, dtype=complex).reshape(no.value, ni.value))
+    S = np.zeros((max(no.value, 1), max(ni.value, 1)), dtype=complex, order="F")
+    g = np.zeros((nx, ny, nz), dtype=complex, order="F")
+    Dp = Dm if Dm.size else np.zeros((1, 1), dtype=complex, order="F")
+    opt = _options(options)
+    check(h.lib.rgf_smatrix_grad_3d(h.h, ctypes.byref(sy), ctypes.byref(req), ctypes.byref(opt), Dp.ctypes.data,
+                                    max(no.value, 1), S.ctypes.data, S.shape[0], g.ctypes.data, int(checkpoint)))
+    del keep
+    S = S[:no.value, :ni.value] if (no.value and ni.value) else np.zeros((no.value, ni.value))
+    return S, g
+
+
 def _one_sided(epsilon_R) -> bool:
     return epsilon_R is None or (np.isscalar(epsilon_R) and np.isnan(epsilon_R))
 

@@ -248,12 +248,14 @@ __device__ __forceinline__ double2 assemble_elem(const PersistParams& p, int64_t
 }
 
 // Slice boundary on this CTA's tile of W (global memory): probe check
-// (p2 = G_n M_n v against v) and, when eps_next is given, the assembly of the
-// next slice matrix: top-left A_{n+1} - G_n, -Z rows, probe pair
-// p1 = v, p2 = A_{n+1} v - G_n v.  Returns the largest probe residual seen.
+// (p2 = G_n M_n v against v), the snapshot of W after the slice when `snap`
+// is given (same layout as W, probe columns excepted) and, when eps_next is
+// given, the assembly of the next slice matrix: top-left A_{n+1} - G_n, -Z
+// rows, probe pair p1 = v, p2 = A_{n+1} v - G_n v.  Returns the largest probe
+// residual seen.
 template <int BM, int BN>
 __device__ double boundary_pass(const PersistParams& p, int I, int Cq, int tid, int nthreads,
-                                const double2* eps_next) {
+                                const double2* eps_next, double2* snap) {
   double pmax = 0.0;
   const int64_t r0 = (int64_t)I * BM, c0 = (int64_t)Cq * BN;
   const int pc1 = p.pc1;
@@ -285,7 +287,10 @@ __device__ double boundary_pass(const PersistParams& p, int I, int Cq, int tid, 
       }
       continue;
     }
-    if (eps_next) __stcg(w, assemble_elem(p, i, j, __ldcg(w), eps_next));
+    if (!eps_next && !snap) continue;
+    const double2 v = __ldcg(w);
+    if (snap) __stcg(snap + i * p.ldm + j, v);
+    if (eps_next) __stcg(w, assemble_elem(p, i, j, v, eps_next));
   }
   return pmax;
 }
@@ -631,7 +636,9 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
       store_tile();
       bar_sync(kBarMath, kMathThreads);
       const double2* eps_next = slice_end ? p.eps + (p.eps_first + (int64_t)(n + 1) * p.eps_step) * p.N : nullptr;
-      probe_max = fmax(probe_max, boundary_pass<BM, BN>(p, I, Cq, tid, kMathThreads, eps_next));
+      double2* snap = (p.snap && (n % p.snap_mod) == p.snap_mod - 1) ? p.snap + (int64_t)(n / p.snap_mod) * p.snap_ld
+                                                                     : nullptr;
+      probe_max = fmax(probe_max, boundary_pass<BM, BN>(p, I, Cq, tid, kMathThreads, eps_next, snap));
       bar_sync(kBarMath, kMathThreads);
       if (slice_end) {
         load_tile();

@@ -25,6 +25,12 @@ struct PersistParams {
   double2* srvbuf;       // [2][32][32] block the T-server updates into the next pivot block
   int* flags;            // pc[TR], row[TC], t[1], u[TC*TR], d[1], srv[2], d_used[1]  (init -1)
   int* cons;             // pc[2][TR], row[2][TC], t[2], u[2][TC], srv[2]             (init 0)
+  // optional snapshots of W after slice n (launch-relative) for every n with
+  // n % snap_mod == snap_mod - 1, at snap + (n / snap_mod) * snap_ld, laid
+  // out as M (probe columns excepted)
+  double2* snap;
+  int snap_mod;
+  int64_t snap_ld;
   int* status;           // kStatus* bits
   int* abort;            // raised by the first wait that times out
   unsigned long long* probe_max;  // bits of max |G_n M_n v - v| (non-negative double)

@@ -59,6 +59,7 @@ struct rgf_handle_s {
   DevBuf k0, k1, kx[2], lam[2], mu[2], isprop[2], prop[2], conj[2], nprop, status;
   DevBuf phi, tmp, g0s, g0e, st_col, st_val, eps, aug, pc, u, idx, sdev;
   DevBuf xpc, xrow, xt, xu, xsync, xprobe, xtrace;  // persistent-kernel exchange buffers
+  DevBuf gck, gseg, gm0, gpsi, gphi, get, gd, gg;   // permittivity gradient (checkpoints, carriers)
   int sms = 0;
   int64_t launches = 0;
   std::string prof_kernel;
@@ -361,8 +362,18 @@ rgf_status smatrix_sizes(rgf_handle h, const Problem& p, const rgf_request* req,
   return RGF_OK;
 }
 
+// Permittivity gradient request of smatrix(): g[m + n*N] = sum_ab D_ab dS_ab / d eps[m, n]
+// for the weights D (n_out x n_in, column-major, leading dimension ldD, in the
+// row/column order of S); D and g are device pointers when S is.
+struct GradReq {
+  const rgf_cplx* D;
+  int64_t ldD;
+  rgf_cplx* g;
+  int64_t checkpoint;  // slices per recomputed segment (<= 0: ceil(sqrt(L)))
+};
+
 rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const rgf_options* opt, rgf_cplx* S,
-                   int64_t ldS, rgf_channels* ch) {
+                   int64_t ldS, rgf_channels* ch, const GradReq* gr = nullptr) {
   rgf_status st;
   h->launches = 0;
   h->probe = 0.0;
@@ -387,7 +398,17 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
   const int noL = (int)rq.out[0].size(), noR = (int)rq.out[1].size();
   const int niL = (int)rq.in[0].size(), niR = (int)rq.in[1].size();
   const int n_out = noL + noR, n_in = niL + niR;
-  if (n_out == 0 || n_in == 0) return copy_channels_out(h, tr, ci, ch);  // :181-184
+  if (n_out == 0 || n_in == 0) {  // :181-184
+    if (gr && L > 0) {  // S is empty: so is its derivative
+      if (S_dev) RGF_CUDA_TRY(cudaMemsetAsync(gr->g, 0, sizeof(rgf_cplx) * N * L, h->stream));
+      else memset(gr->g, 0, sizeof(rgf_cplx) * N * L);
+    }
+    return copy_channels_out(h, tr, ci, ch);
+  }
+  if (gr && gr->ldD < n_out) {
+    set_error("ldD must be >= the number of requested output channels");
+    return RGF_ERR_ARG;
+  }
   if (!S) {
     set_error("S must not be NULL");
     return RGF_ERR_ARG;
@@ -551,158 +572,182 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
   unsigned long long* probe_d = nullptr;
   h->prof_kernel = sweep_update_kernel_name();
   if (use_persist) {
-    const int TR = (int)((Rp + BMp - 1) / BMp), TC = (int)((Cp + BNp - 1) / BNp);
-    const int nflags = persist_flag_words(TR, TC), ncons = persist_cons_words(TR, TC);
-    if ((st = ensure(h->xpc, sizeof(double2) * 2 * TR * BMp * 32))) return st;
-    if ((st = ensure(h->xrow, sizeof(double2) * 2 * TC * 32 * BNp))) return st;
-    if ((st = ensure(h->xt, sizeof(double2) * 5 * 32 * 32))) return st;  // tbuf[2], djjbuf, srvbuf[2]
-    if ((st = ensure(h->xu, sizeof(double2) * 2 * TC * 32 * BNp))) return st;
-    if ((st = ensure(h->xsync, sizeof(int) * (nflags + ncons + 4)))) return st;
     if ((st = ensure(h->xprobe, sizeof(unsigned long long)))) return st;
-    int* flags = as<int>(h->xsync);
-    RGF_CUDA_TRY(cudaMemsetAsync(flags, 0xFF, sizeof(int) * nflags, h->stream));
-    RGF_CUDA_TRY(cudaMemsetAsync(flags + nflags, 0, sizeof(int) * (ncons + 4), h->stream));
     probe_d = as<unsigned long long>(h->xprobe);
     RGF_CUDA_TRY(cudaMemsetAsync(probe_d, 0, sizeof(unsigned long long), h->stream));
-    launch_probe_init(M, ldm, N, Rp, pc1, h->stream);
-    h->launches++;
-    PersistParams pp;
-    pp.N = (int)N;
-    pp.R = (int)Rp;
-    pp.C = (int)Cp;
-    pp.TR = TR;
-    pp.TC = TC;
-    pp.NB = (int)((N + kSwW - 1) / kSwW);
-    pp.L = (int)L;
-    pp.M = M;
-    pp.ldm = ldm;
-    pp.eps = eps_d;
-    pp.eps_first = mirror ? L - 1 : 0;
-    pp.eps_step = mirror ? -1 : 1;
-    pp.k2 = k2;
-    pp.st_col = st_col;
-    pp.st_val = st_val;
-    pp.pc1 = (int)pc1;
-    pp.pcbuf = as<double2>(h->xpc);
-    pp.rowbuf = as<double2>(h->xrow);
-    pp.tbuf = as<double2>(h->xt);
-    pp.djjbuf = as<double2>(h->xt) + 2 * 32 * 32;
-    pp.srvbuf = as<double2>(h->xt) + 3 * 32 * 32;
-    pp.ubuf = as<double2>(h->xu);
-    pp.flags = flags;
-    pp.cons = flags + nflags;
-    pp.abort = flags + nflags + ncons;
-    pp.status = status;
-    pp.probe_max = probe_d;
-    int clk_khz = 2000000;
-    cudaDeviceGetAttribute(&clk_khz, cudaDevAttrClockRate, h->device);
-    pp.timeout_cycles = (long long)clk_khz * 1000LL * 4;  // ~4 s per wait
-    // RGF_TRACE=<file>: record per-step role timestamps of the first
-    // RGF_TRACE_STEPS (default 128) steps.  RGF_WATCH=<seconds> (with
-    // RGF_TRACE): if the launch is still running after that long, the trace
-    // recorded so far is read through a second stream and written, and the
-    // call fails with RGF_ERR_TIMEOUT.
-    const char* trace_path = getenv("RGF_TRACE");
-    const char* watch_env = getenv("RGF_WATCH");
-    const char* steps_env = getenv("RGF_TRACE_STEPS");
-    pp.trace = nullptr;
-    pp.trace_steps = 0;
-    if (trace_path && *trace_path) {
-      pp.trace_steps = steps_env ? std::max(1, std::min(atoi(steps_env), (int)(L * pp.NB))) : 128;
-      if ((st = ensure(h->xtrace, sizeof(unsigned long long) * (size_t)(TR * TC + 1) * pp.trace_steps * kTraceEvents)))
-        return st;
-      pp.trace = as<unsigned long long>(h->xtrace);
-      RGF_CUDA_TRY(cudaMemsetAsync(pp.trace, 0, h->xtrace.bytes, h->stream));
-    }
-    const bool timed = prof_every > 0;
-    if (timed) {
-      while (h->ev.size() < 2) {
-        cudaEvent_t ev;
-        RGF_CUDA_TRY(cudaEventCreate(&ev));
-        h->ev.push_back(ev);
-      }
-      RGF_CUDA_TRY(cudaEventRecord(h->ev[0], h->stream));
-    }
-    cudaError_t e = launch_persist(pp, BMp, BNp, h->stream);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      use_persist = false;  // e.g. the cooperative launch does not fit: per-step engine below
-      probe_d = nullptr;
-    } else {
+  }
+  // Sweeps the slices [k_lo, k_hi) of the recursion order.  On entry M holds
+  // the assembled matrix of slice k_lo, on return W after slice k_hi - 1 (not
+  // assembled).  With `snap`, W after every slice k with
+  // (k - k_lo) % snap_mod == snap_mod - 1 is also copied to
+  // snap + ((k - k_lo) / snap_mod) * Rp * ldm.
+  auto run_slices = [&](int64_t k_lo, int64_t k_hi, double2* snap, int snap_mod) -> rgf_status {
+    const int64_t nsl = k_hi - k_lo;
+    if (use_persist) {
+      const int TR = (int)((Rp + BMp - 1) / BMp), TC = (int)((Cp + BNp - 1) / BNp);
+      const int nflags = persist_flag_words(TR, TC), ncons = persist_cons_words(TR, TC);
+      if ((st = ensure(h->xpc, sizeof(double2) * 2 * TR * BMp * 32))) return st;
+      if ((st = ensure(h->xrow, sizeof(double2) * 2 * TC * 32 * BNp))) return st;
+      if ((st = ensure(h->xt, sizeof(double2) * 5 * 32 * 32))) return st;  // tbuf[2], djjbuf, srvbuf[2]
+      if ((st = ensure(h->xu, sizeof(double2) * 2 * TC * 32 * BNp))) return st;
+      if ((st = ensure(h->xsync, sizeof(int) * (nflags + ncons + 4)))) return st;
+      int* flags = as<int>(h->xsync);
+      RGF_CUDA_TRY(cudaMemsetAsync(flags, 0xFF, sizeof(int) * nflags, h->stream));
+      RGF_CUDA_TRY(cudaMemsetAsync(flags + nflags, 0, sizeof(int) * (ncons + 4), h->stream));
+      launch_probe_init(M, ldm, N, Rp, pc1, h->stream);
       h->launches++;
+      PersistParams pp;
+      pp.N = (int)N;
+      pp.R = (int)Rp;
+      pp.C = (int)Cp;
+      pp.TR = TR;
+      pp.TC = TC;
+      pp.NB = (int)((N + kSwW - 1) / kSwW);
+      pp.L = (int)nsl;
+      pp.M = M;
+      pp.ldm = ldm;
+      pp.eps = eps_d;
+      pp.eps_first = mirror ? L - 1 - k_lo : k_lo;
+      pp.eps_step = mirror ? -1 : 1;
+      pp.k2 = k2;
+      pp.st_col = st_col;
+      pp.st_val = st_val;
+      pp.pc1 = (int)pc1;
+      pp.pcbuf = as<double2>(h->xpc);
+      pp.rowbuf = as<double2>(h->xrow);
+      pp.tbuf = as<double2>(h->xt);
+      pp.djjbuf = as<double2>(h->xt) + 2 * 32 * 32;
+      pp.srvbuf = as<double2>(h->xt) + 3 * 32 * 32;
+      pp.ubuf = as<double2>(h->xu);
+      pp.flags = flags;
+      pp.cons = flags + nflags;
+      pp.abort = flags + nflags + ncons;
+      pp.snap = snap;
+      pp.snap_mod = snap ? snap_mod : 1;
+      pp.snap_ld = Rp * ldm;
+      pp.status = status;
+      pp.probe_max = probe_d;
+      int clk_khz = 2000000;
+      cudaDeviceGetAttribute(&clk_khz, cudaDevAttrClockRate, h->device);
+      pp.timeout_cycles = (long long)clk_khz * 1000LL * 4;  // ~4 s per wait
+      // RGF_TRACE=<file>: record per-step role timestamps of the first
+      // RGF_TRACE_STEPS (default 128) steps of the first launch.
+      // RGF_WATCH=<seconds> (with RGF_TRACE): if that launch is still running
+      // after that long, the trace recorded so far is read through a second
+      // stream and written, and the call fails with RGF_ERR_TIMEOUT.
+      const char* trace_path = k_lo == 0 ? getenv("RGF_TRACE") : nullptr;
+      const char* watch_env = getenv("RGF_WATCH");
+      const char* steps_env = getenv("RGF_TRACE_STEPS");
+      pp.trace = nullptr;
+      pp.trace_steps = 0;
+      if (trace_path && *trace_path) {
+        pp.trace_steps = steps_env ? std::max(1, std::min(atoi(steps_env), (int)(nsl * pp.NB))) : 128;
+        if ((st = ensure(h->xtrace,
+                         sizeof(unsigned long long) * (size_t)(TR * TC + 1) * pp.trace_steps * kTraceEvents)))
+          return st;
+        pp.trace = as<unsigned long long>(h->xtrace);
+        RGF_CUDA_TRY(cudaMemsetAsync(pp.trace, 0, h->xtrace.bytes, h->stream));
+      }
+      const bool timed = prof_every > 0;
       if (timed) {
-        RGF_CUDA_TRY(cudaEventRecord(h->ev[1], h->stream));
-        ev_used = 2;
-        for (int64_t j0 = 0; j0 < N; j0 += kSwW)
-          prof_flops += (double)L * 8.0 * (double)Rp * (double)(N + ni_s) * (double)std::min<int64_t>(kSwW, N - j0);
-      }
-      char nm[64];
-      snprintf(nm, sizeof(nm), "k_persist<%d,%d> (FP64 DMMA sweep, all slices)", BMp, BNp);
-      h->prof_kernel = nm;
-      bool hung = false;
-      if (pp.trace && watch_env && atof(watch_env) > 0) {
-        const auto t_start = std::chrono::steady_clock::now();
-        for (;;) {
-          const cudaError_t q = cudaStreamQuery(h->stream);
-          if (q == cudaSuccess) break;
-          if (q != cudaErrorNotReady) RGF_CUDA_TRY(q);
-          const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
-          if (el > atof(watch_env)) {
-            hung = true;
-            break;
-          }
-          std::this_thread::sleep_for(std::chrono::milliseconds(10));
+        while (h->ev.size() < ev_used + 2) {
+          cudaEvent_t ev;
+          RGF_CUDA_TRY(cudaEventCreate(&ev));
+          h->ev.push_back(ev);
         }
+        RGF_CUDA_TRY(cudaEventRecord(h->ev[ev_used], h->stream));
       }
-      if (pp.trace) {
-        std::vector<unsigned long long> tr((size_t)(TR * TC + 1) * pp.trace_steps * kTraceEvents);
-        if (hung) {
-          cudaStream_t side;
-          RGF_CUDA_TRY(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
-          RGF_CUDA_TRY(cudaMemcpyAsync(tr.data(), pp.trace, sizeof(unsigned long long) * tr.size(),
-                                       cudaMemcpyDeviceToHost, side));
-          std::vector<int> words(nflags + ncons + 1);
-          RGF_CUDA_TRY(cudaMemcpyAsync(words.data(), flags, sizeof(int) * words.size(), cudaMemcpyDeviceToHost, side));
-          RGF_CUDA_TRY(cudaStreamSynchronize(side));
-          const std::string wpath = std::string(trace_path) + ".flags";
-          if (FILE* fw = fopen(wpath.c_str(), "wb")) {
-            fwrite(words.data(), sizeof(int), words.size(), fw);
-            fclose(fw);
+      cudaError_t e = launch_persist(pp, BMp, BNp, h->stream);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        use_persist = false;  // e.g. the cooperative launch does not fit: per-step engine below
+        probe_d = nullptr;
+      } else {
+        h->launches++;
+        if (timed) {
+          RGF_CUDA_TRY(cudaEventRecord(h->ev[ev_used + 1], h->stream));
+          ev_used += 2;
+          for (int64_t j0 = 0; j0 < N; j0 += kSwW)
+            prof_flops +=
+                (double)nsl * 8.0 * (double)Rp * (double)(N + ni_s) * (double)std::min<int64_t>(kSwW, N - j0);
+        }
+        char nm[64];
+        snprintf(nm, sizeof(nm), "k_persist<%d,%d> (FP64 DMMA sweep, all slices)", BMp, BNp);
+        h->prof_kernel = nm;
+        bool hung = false;
+        if (pp.trace && watch_env && atof(watch_env) > 0) {
+          const auto t_start = std::chrono::steady_clock::now();
+          for (;;) {
+            const cudaError_t q = cudaStreamQuery(h->stream);
+            if (q == cudaSuccess) break;
+            if (q != cudaErrorNotReady) RGF_CUDA_TRY(q);
+            const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+            if (el > atof(watch_env)) {
+              hung = true;
+              break;
+            }
+            std::this_thread::sleep_for(std::chrono::milliseconds(10));
           }
-          FILE* f = fopen(trace_path, "wb");
-          if (f) {
+        }
+        if (pp.trace) {
+          std::vector<unsigned long long> tr((size_t)(TR * TC + 1) * pp.trace_steps * kTraceEvents);
+          cudaStream_t rd = h->stream;
+          if (hung) RGF_CUDA_TRY(cudaStreamCreateWithFlags(&rd, cudaStreamNonBlocking));
+          RGF_CUDA_TRY(cudaMemcpyAsync(tr.data(), pp.trace, sizeof(unsigned long long) * tr.size(),
+                                       cudaMemcpyDeviceToHost, rd));
+          std::vector<int> words(nflags + ncons + 1);
+          if (hung)
+            RGF_CUDA_TRY(
+                cudaMemcpyAsync(words.data(), flags, sizeof(int) * words.size(), cudaMemcpyDeviceToHost, rd));
+          RGF_CUDA_TRY(cudaStreamSynchronize(rd));
+          if (hung) {
+            const std::string wpath = std::string(trace_path) + ".flags";
+            if (FILE* fw = fopen(wpath.c_str(), "wb")) {
+              fwrite(words.data(), sizeof(int), words.size(), fw);
+              fclose(fw);
+            }
+          }
+          if (FILE* f = fopen(trace_path, "wb")) {
             int hdr[4] = {TR, TC, pp.trace_steps, (int)kTraceEvents};
             fwrite(hdr, sizeof(int), 4, f);
             fwrite(tr.data(), sizeof(unsigned long long), tr.size(), f);
             fclose(f);
           }
-          set_error("persistent sweep still running after RGF_WATCH seconds; trace written");
-          return RGF_ERR_TIMEOUT;
+          if (hung) {
+            set_error("persistent sweep still running after RGF_WATCH seconds; trace written");
+            return RGF_ERR_TIMEOUT;
+          }
         }
-        RGF_CUDA_TRY(cudaMemcpyAsync(tr.data(), pp.trace, sizeof(unsigned long long) * tr.size(),
-                                     cudaMemcpyDeviceToHost, h->stream));
-        RGF_CUDA_TRY(cudaStreamSynchronize(h->stream));
-        FILE* f = fopen(trace_path, "wb");
-        if (f) {
-          int hdr[4] = {TR, TC, pp.trace_steps, (int)kTraceEvents};
-          fwrite(hdr, sizeof(int), 4, f);
-          fwrite(tr.data(), sizeof(unsigned long long), tr.size(), f);
-          fclose(f);
-        }
+        return RGF_OK;
       }
-      attach(false);
     }
+    for (int64_t k = k_lo; k < k_hi; k++) {
+      if ((st = sweep(N + no_s, N + ni_s, prof_every && (k % prof_every) == 0))) return st;
+      if (snap && (k - k_lo) % snap_mod == snap_mod - 1)
+        RGF_CUDA_TRY(cudaMemcpyAsync(snap + ((k - k_lo) / snap_mod) * Rp * ldm, M, sizeof(double2) * Rp * ldm,
+                                     cudaMemcpyDeviceToDevice, h->stream));
+      if (k + 1 < k_hi) {
+        launch_assemble(M, ldm, N, N + no_s, M, ldm, nullptr, 0, st_col, st_val, k2, slice_eps(k + 1), cmk(0, 0),
+                        h->stream);
+        h->launches++;
+      }
+      if (((k + 1) & 63) == 0 && (st = check_launch())) return st;
+    }
+    return RGF_OK;
+  };
+  // gradient: checkpoints of the forward sweep (W after every K-th slice) and
+  // the assembled first slice
+  const int64_t gK = gr ? (gr->checkpoint > 0 ? std::min<int64_t>(gr->checkpoint, std::max<int64_t>(L, 1))
+                                              : std::max<int64_t>(1, (int64_t)ceil(sqrt((double)L))))
+                        : 0;
+  if (gr && L > 0) {
+    if ((st = ensure(h->gck, sizeof(double2) * Rp * ldm * std::max<int64_t>(1, L / gK)))) return st;
+    if ((st = ensure(h->gm0, sizeof(double2) * Rp * ldm))) return st;
+    RGF_CUDA_TRY(cudaMemcpyAsync(h->gm0.p, M, sizeof(double2) * Rp * ldm, cudaMemcpyDeviceToDevice, h->stream));
   }
-  for (int64_t k = 0; !use_persist && k < L; k++) {
-    if ((st = sweep(N + no_s, N + ni_s, prof_every && (k % prof_every) == 0))) return st;
-    if (k + 1 < L) {
-      launch_assemble(M, ldm, N, N + no_s, M, ldm, nullptr, 0, st_col, st_val, k2, slice_eps(k + 1), cmk(0, 0),
-                      h->stream);
-      h->launches++;
-    } else {
-      attach(false);
-    }
-    if (((k + 1) & 63) == 0 && (st = check_launch())) return st;
+  if (L > 0) {
+    if ((st = run_slices(0, L, gr ? as<double2>(h->gck) : nullptr, (int)gK))) return st;
+    attach(false);
   }
   if ((st = sweep(R, C, false))) return st;
 
@@ -717,6 +762,80 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
     RGF_CUDA_TRY(cudaMemcpy2DAsync(S, sizeof(rgf_cplx) * ldS, Sd, sizeof(double2) * n_out,
                                    sizeof(double2) * n_out, n_in, cudaMemcpyDeviceToHost, h->stream));
   }
+  // (9) permittivity gradient: the backward recursions
+  //     Psi_j = [X_j, 0] + g_j Psi_{j+1},  Phi_j = [Z_j; 0] + Phi_{j+1} g_j
+  //     dS_ab/d eps(m, slice j) = -2i k0dx^2 Phi_j[a][m] Psi_j[m][b]
+  //     over the start-connected blocks g_j and carriers X_j, Z_j of the
+  //     sweep, segment by segment from the last: each segment's slices are
+  //     recomputed from its checkpoint with a snapshot after every slice.
+  if (gr && L > 0) {
+    const int64_t nI = n_in, nO = n_out;
+    std::vector<rgf_cplx> Du((size_t)nO * nI), Da((size_t)nO * nI);
+    if (S_dev) {
+      RGF_CUDA_TRY(cudaMemcpy2DAsync(Du.data(), sizeof(rgf_cplx) * nO, gr->D, sizeof(rgf_cplx) * gr->ldD,
+                                     sizeof(rgf_cplx) * nO, nI, cudaMemcpyDeviceToHost, h->stream));
+      RGF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    } else {
+      for (int64_t i = 0; i < nI; i++)
+        for (int64_t o = 0; o < nO; o++) Du[o + i * nO] = gr->D[o + i * gr->ldD];
+    }
+    for (int64_t i = 0; i < nI; i++)
+      for (int64_t o = 0; o < nO; o++) Da[(size_t)row_of[o] * nI + col_of[i]] = Du[o + i * nO];
+    if ((st = ensure(h->gd, sizeof(double2) * nO * nI))) return st;
+    if ((st = ensure(h->gpsi, sizeof(double2) * 2 * N * nI))) return st;
+    if ((st = ensure(h->gphi, sizeof(double2) * 2 * nO * N))) return st;
+    if ((st = ensure(h->get, sizeof(double2) * nO * N))) return st;
+    if ((st = ensure(h->gseg, sizeof(double2) * gK * Rp * ldm))) return st;
+    if (!S_dev && (st = ensure(h->gg, sizeof(double2) * N * L))) return st;
+    double2* Dd = as<double2>(h->gd);
+    RGF_CUDA_TRY(cudaMemcpyAsync(Dd, Da.data(), sizeof(double2) * nO * nI, cudaMemcpyHostToDevice, h->stream));
+    double2* psi[2] = {as<double2>(h->gpsi), as<double2>(h->gpsi) + N * nI};
+    double2* phv[2] = {as<double2>(h->gphi), as<double2>(h->gphi) + nO * N};
+    double2* Et = as<double2>(h->get);
+    double2* seg = as<double2>(h->gseg);
+    double2* gout = S_dev ? reinterpret_cast<double2*>(gr->g) : as<double2>(h->gg);
+    // Psi_{L+1} = W(0:N, N:N+n_in) and Phi_{L+1} = W(N:N+n_out, 0:N) after the far lead
+    RGF_CUDA_TRY(cudaMemcpy2DAsync(psi[0], sizeof(double2) * nI, M + N, sizeof(double2) * ldm, sizeof(double2) * nI,
+                                   N, cudaMemcpyDeviceToDevice, h->stream));
+    RGF_CUDA_TRY(cudaMemcpy2DAsync(phv[0], sizeof(double2) * N, M + N * ldm, sizeof(double2) * ldm,
+                                   sizeof(double2) * N, nO, cudaMemcpyDeviceToDevice, h->stream));
+    const double2 coef = cmul(cmk(0.0, -2.0), k2);
+    const double2 one = cmk(1.0, 0.0), zero = cmk(0.0, 0.0);
+    int cur = 0;
+    const int64_t nseg = (L + gK - 1) / gK;
+    for (int64_t sg = nseg - 1; sg >= 0; sg--) {
+      const int64_t k_lo = sg * gK, k_hi = std::min(L, k_lo + gK);
+      if (sg == 0) {
+        RGF_CUDA_TRY(cudaMemcpyAsync(M, h->gm0.p, sizeof(double2) * Rp * ldm, cudaMemcpyDeviceToDevice, h->stream));
+      } else {
+        RGF_CUDA_TRY(cudaMemcpyAsync(M, as<double2>(h->gck) + (sg - 1) * Rp * ldm, sizeof(double2) * Rp * ldm,
+                                     cudaMemcpyDeviceToDevice, h->stream));
+        launch_assemble(M, ldm, N, N + no_s, M, ldm, nullptr, 0, st_col, st_val, k2, slice_eps(k_lo), cmk(0, 0),
+                        h->stream);
+        h->launches++;
+      }
+      if ((st = run_slices(k_lo, k_hi, seg, 1))) return st;
+      for (int64_t j = k_hi - 1; j >= k_lo; j--) {
+        const double2* Wj = seg + (j - k_lo) * Rp * ldm;
+        const int nx_ = cur ^ 1;
+        launch_copy_pad(psi[nx_], nI, N, nI, Wj + N, ldm, N, ni_s, h->stream);
+        launch_zgemm(N, nI, N, one, ZOp{Wj, ldm, 0}, ZOp{psi[cur], nI, 0}, one, psi[nx_], nI, h->stream);
+        launch_copy_pad(phv[nx_], N, nO, N, Wj + N * ldm, ldm, no_s, N, h->stream);
+        launch_zgemm(nO, N, N, one, ZOp{phv[cur], N, 0}, ZOp{Wj, ldm, 0}, one, phv[nx_], N, h->stream);
+        launch_zgemm(nO, N, nI, one, ZOp{Dd, nI, 0}, ZOp{psi[nx_], nI, 1}, zero, Et, N, h->stream);
+        const int64_t n_phys = mirror ? L - 1 - j : j;
+        launch_grad_slice(phv[nx_], Et, N, nO, coef, gout + n_phys * N, h->stream);
+        h->launches += 6;
+        cur = nx_;
+      }
+      if ((st = check_launch())) return st;
+    }
+    if (!S_dev)
+      RGF_CUDA_TRY(cudaMemcpyAsync(gr->g, gout, sizeof(double2) * N * L, cudaMemcpyDeviceToHost, h->stream));
+  } else if (gr) {
+    // no slices: nothing depends on epsilon
+  }
+
   int hstatus = 0;
   unsigned long long probe_bits = 0;
   RGF_CUDA_TRY(cudaMemcpyAsync(&hstatus, status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
@@ -871,7 +990,9 @@ rgf_status rgf_destroy(rgf_handle h) {
                     &h->conj[0], &h->conj[1], &h->nprop,   &h->status,    &h->phi,     &h->tmp,
                     &h->g0s,    &h->g0e,    &h->st_col,    &h->st_val,    &h->eps,     &h->aug,
                     &h->pc,     &h->u,      &h->idx,       &h->sdev,      &h->xpc,     &h->xrow,
-                    &h->xt,     &h->xu,     &h->xsync,     &h->xprobe,    &h->xtrace};
+                    &h->xt,     &h->xu,     &h->xsync,     &h->xprobe,    &h->xtrace,  &h->gck,
+                    &h->gseg,   &h->gm0,    &h->gpsi,      &h->gphi,      &h->get,     &h->gd,
+                    &h->gg};
   for (DevBuf* b : bufs)
     if (b->p) cudaFree(b->p);
   for (cudaEvent_t ev : h->ev) cudaEventDestroy(ev);
@@ -900,6 +1021,32 @@ rgf_status rgf_smatrix_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_reques
     return RGF_ERR_ARG;
   }
   return smatrix(h, problem3d(syst), req, opt, S, ldS, ch);
+}
+
+rgf_status rgf_smatrix_grad_2d(rgf_handle h, const rgf_syst2d* syst, const rgf_request* req,
+                               const rgf_options* opt, const rgf_cplx* D, int64_t ldD, rgf_cplx* S, int64_t ldS,
+                               rgf_cplx* g, int64_t checkpoint) {
+  rgf_status st;
+  if ((st = check_handle(h))) return st;
+  if (!syst || !D || !g) {
+    set_error("syst, D and g must not be NULL");
+    return RGF_ERR_ARG;
+  }
+  GradReq gr{D, ldD, g, checkpoint};
+  return smatrix(h, problem2d(syst), req, opt, S, ldS, nullptr, &gr);
+}
+
+rgf_status rgf_smatrix_grad_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_request* req,
+                               const rgf_options* opt, const rgf_cplx* D, int64_t ldD, rgf_cplx* S, int64_t ldS,
+                               rgf_cplx* g, int64_t checkpoint) {
+  rgf_status st;
+  if ((st = check_handle(h))) return st;
+  if (!syst || !D || !g) {
+    set_error("syst, D and g must not be NULL");
+    return RGF_ERR_ARG;
+  }
+  GradReq gr{D, ldD, g, checkpoint};
+  return smatrix(h, problem3d(syst), req, opt, S, ldS, nullptr, &gr);
 }
 
 rgf_status rgf_smatrix_size_2d(rgf_handle h, const rgf_syst2d* syst, const rgf_request* req, int64_t* n_out,

@@ -478,4 +478,39 @@ void launch_scale_cols(const double2* src, int64_t lds, const double2* diag, dou
   k_scale_cols<<<grid, 128, 0, s>>>(src, lds, diag, dst, ldd, rows, cols);
 }
 
+// ---------------------------------------------------------------------------
+// permittivity gradient
+// ---------------------------------------------------------------------------
+// dst (rows x cols, row-major, ld ldd) = src in its top-left src_rows x
+// src_cols corner, zero elsewhere
+__global__ void k_copy_pad(double2* dst, int64_t ldd, int64_t rows, int64_t cols, const double2* src, int64_t lds,
+                           int64_t src_rows, int64_t src_cols) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  for (int64_t r = blockIdx.y; r < rows; r += gridDim.y)
+    dst[r * ldd + c] = (r < src_rows && c < src_cols) ? src[r * lds + c] : cmk(0.0, 0.0);
+}
+
+void launch_copy_pad(double2* dst, int64_t ldd, int64_t rows, int64_t cols, const double2* src, int64_t lds,
+                     int64_t src_rows, int64_t src_cols, cudaStream_t s) {
+  if (rows <= 0 || cols <= 0) return;
+  dim3 grid((unsigned)((cols + 127) / 128), (unsigned)(rows < 4096 ? rows : 4096));
+  k_copy_pad<<<grid, 128, 0, s>>>(dst, ldd, rows, cols, src, lds, src_rows, src_cols);
+}
+
+// g[m] = coef * sum_a Phi[a][m] Et[a][m]  (Phi, Et: n_out x N row-major)
+__global__ void k_grad_slice(const double2* Phi, const double2* Et, int64_t N, int64_t n_out, double2 coef,
+                             double2* g) {
+  const int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (m >= N) return;
+  double2 acc = cmk(0.0, 0.0);
+  for (int64_t a = 0; a < n_out; a++) acc = cadd(acc, cmul(Phi[a * N + m], Et[a * N + m]));
+  g[m] = cmul(coef, acc);
+}
+
+void launch_grad_slice(const double2* Phi, const double2* Et, int64_t N, int64_t n_out, double2 coef, double2* g,
+                       cudaStream_t s) {
+  k_grad_slice<<<(unsigned)((N + 127) / 128), 128, 0, s>>>(Phi, Et, N, n_out, coef, g);
+}
+
 }  // namespace rgf

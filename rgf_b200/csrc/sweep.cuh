@@ -35,5 +35,11 @@ void launch_probe_init(double2* M, int64_t ldm, int64_t N, int64_t R, int64_t pc
 void launch_check_finite(const double2* x, int64_t n, int* status, cudaStream_t s);
 void launch_scale_cols(const double2* src, int64_t lds, const double2* diag, double2* dst, int64_t ldd,
                        int64_t rows, int64_t cols, cudaStream_t s);
+// permittivity gradient: zero-padded copy and the per-slice contraction
+// g[m] = coef * sum_a Phi[a][m] Et[a][m]
+void launch_copy_pad(double2* dst, int64_t ldd, int64_t rows, int64_t cols, const double2* src, int64_t lds,
+                     int64_t src_rows, int64_t src_cols, cudaStream_t s);
+void launch_grad_slice(const double2* Phi, const double2* Et, int64_t N, int64_t n_out, double2 coef, double2* g,
+                       cudaStream_t s);
 
 }  // namespace rgf
