@@ -46,6 +46,7 @@ METRIC = "S-matrices/s 2D N=1024 L=4096: 3xTF32+refine vs FP64 at 1e-10 rel err;
 UNIT = "S-matrices/s"
 FP64_DMMA_FALLBACK_TFLOPS = 37.0  # earlier measurement on this pool, used only if the live one fails
 PROFILE_EVERY = 64
+DRAM_BYTES_PER_SLICE = (20.993536e6 + 9.418240e6) / 16  # k_persist<96,96>, config 2, ncu over 16 slices
 
 
 def log(*a):
@@ -355,10 +356,10 @@ def run_ours(args, dist):
     n, ms, fl_exec, name = prof
     fl = nx * workloads.canonical_slice_flops(ny, n_in // 2, n_out // 2)  # the launch covers all nx slices
     achieved = fl / (ms / n / 1e3) / 1e12 if n else None
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get("sweep_update_bytes_per_launch")
+    # DRAM bytes (read + write) of one k_persist launch: the ncu capture of the
+    # first 16 slices (profiles/k_persist_config2_16slices.md) scaled to the
+    # launch's slice count (the traffic per slice is constant)
+    traffic = DRAM_BYTES_PER_SLICE * nx
     line["roofline"] = {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": peak,
                         "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
                         "traffic": traffic, "flops_per_launch": fl, "executed_flops_per_launch": fl_exec,
