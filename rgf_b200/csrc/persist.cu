@@ -102,22 +102,21 @@ __device__ __forceinline__ unsigned long long gtimer() {
   return t;
 }
 
-// 1/z = conj(z) / |z|^2 with the real reciprocal 1/n refined by two
-// Newton-Raphson steps r <- r + r (1 - n r) from a single-precision seed
-// (quadratic convergence: ~24 -> ~48 -> full double precision); IEEE
-// division outside the single-precision range
-__device__ __forceinline__ double2 crecip(double2 z) {
-  const double n = z.x * z.x + z.y * z.y;
-  double r;
-  if (n > 1e-30 && n < 1e30) {
-    r = (double)(1.0f / (float)n);
-    double e = fma(-n, r, 1.0);
-    r = fma(r, e, r);
-    e = fma(-n, r, 1.0);
-    r = fma(r, e, r);
-  } else {
-    r = 1.0 / n;
-  }
+// 1/z = conj(z) / |z|^2 with the real reciprocal r = 1/n from the
+// single-precision approximation (rcp.approx) refined by two Newton-Raphson
+// steps r <- r + r (1 - n r) (quadratic convergence: ~23 -> ~46 -> full
+// double precision).  Branch-free: n is clamped to [1e-30, 1e30] so that
+// every lane of a warp can form it speculatively; pivots outside that range
+// are handled by the caller.
+__device__ __forceinline__ double2 crecip_fast(double2 z) {
+  const double n = fmin(fmax(z.x * z.x + z.y * z.y, 1e-30), 1e30);
+  float rf;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rf) : "f"((float)n));
+  double r = (double)rf;
+  double e = fma(-n, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-n, r, 1.0);
+  r = fma(r, e, r);
   return cmk(z.x * r, -z.y * r);
 }
 
@@ -144,7 +143,7 @@ struct Shared {
   int panel_abort;
   Blk T;   // panel role: T_s
   Blk Mr;  // panel role: my columns of the pivot rows
-  double2 fcol[2][kPB];
+  double2 fcol[2][kPB];   // T-server Gauss-Jordan: pivot column, reciprocal and row of a step
   double2 dpiv[2];
   int piv[2];
   int perm[kPB], pinv[kPB];
@@ -430,7 +429,6 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
     const int n = pub_set(kSetDjj, s1, &lead);
     const int all_ok = !bar_or(kBarDjj, n * 32, !ok);
     if (warp == lead && t.lane == 0 && all_ok) {
-      __threadfence();
       st_release(sy.d_flag, s1);
     }
   };
@@ -491,7 +489,6 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
     if (warp == lead && t.lane == 0) trace_ev(p, s1 - 1, kTrGlobStored);
     const int all_ok = !bar_or(kBarPub, n * 32, !ok);
     if (warp == lead && t.lane == 0 && all_ok) {  // an aborted publish never releases anything
-      __threadfence();
       if (w0 >= tr0 && w0 < tr0 + BM) st_release(sy.row_flag + Cq, s1);
       if (w0 >= tc0 && w0 < tc0 + BN) st_release(sy.pc_flag + I, s1);
       trace_ev(p, s1 - 1, kTrMathPublished);
@@ -516,7 +513,6 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
     if (warp == lead && t.lane == 0) trace_ev(p, s1 - 1, kTrSrvPubStored);
     const int all_ok = !bar_or(kBarSrv, n * 32, !ok);
     if (warp == lead && t.lane == 0 && all_ok) {
-      __threadfence();
       st_release(sy.srv_flag + par, s2);
       trace_ev(p, s1 - 1, kTrSrvPubDone);
     }
@@ -724,7 +720,6 @@ __device__ void panel_role(const PersistParams& p, Shared& sh, const Sync& sy, i
     if (t == 0) {
       atomicAdd(sy.t_cons + par, 1);
       atomicAdd(sy.row_cons + par * p.TC + Cq, 1);
-      __threadfence();
       st_release(sy.u_flag + Cq * p.TR + I, s);
       trace_ev(p, s, kTrPanelUout);
     }
@@ -755,14 +750,19 @@ __device__ __forceinline__ void gj_block(const PersistParams& p, Shared& sh, dou
       double2 vq = a[0];
 #pragma unroll
       for (int c = 1; c < NC; c++) vq = (c == cq) ? a[c] : vq;
-      const double2 dq = crecip(vq);  // speculative: used only if this lane wins
+      const double2 dq = crecip_fast(vq);  // speculative: used only if this lane wins
       const float fx = (float)vq.x, fy = (float)vq.y;
       const float mag = fx * fx + fy * fy;
       const bool elig = (lane < jn) && !((used >> lane) & 1u);
       const unsigned key = elig ? ((__float_as_uint(mag) & ~63u) | (unsigned)(32 - lane)) : 0u;
       const unsigned best = __reduce_max_sync(kFull, key);
       const int pv = 32 - (int)(best & 63u);
-      const double2 d = cmk(__shfl_sync(kFull, dq.x, pv), __shfl_sync(kFull, dq.y, pv));
+      double2 d = cmk(__shfl_sync(kFull, dq.x, pv), __shfl_sync(kFull, dq.y, pv));
+      const float magp = __uint_as_float(best & ~63u);  // the winner's |v|^2 (single precision)
+      if (!(magp >= 1e-29f && magp <= 1e29f)) {          // warp-uniform, rare: exact reciprocal
+        const double2 vp = cmk(__shfl_sync(kFull, vq.x, pv), __shfl_sync(kFull, vq.y, pv));
+        d = cinv(vp);
+      }
       sh.fcol[b][lane] = vq;
       if (lane == 0) {
         sh.piv[b] = pv;
@@ -868,13 +868,21 @@ __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, 
       const int I2 = w / BM, C2 = w / BN;
       const double2* pcb = p.pcbuf + ((size_t)parq * p.TR + I2) * (BM * kPB) + (size_t)(w - I2 * BM) * kPB;
       const double2* rwb = p.rowbuf + ((size_t)parq * p.TC + C2) * (kPB * BN) + (w - C2 * BN);
-      for (int e = t; e < kPB * kPB; e += kServerThreads) {
-        const int r = e / kPB, c = e % kPB;
-        sh.srv.a1[r][c] = __ldcg(sb + e);
-        const double2 pcv = __ldcg(pcb + r * kPB + (c ^ ((r & 1) << 2)));
-        sh.srv.a2[r][c] = r < jn ? cneg(pcv) : cmk(0.0, 0.0);
-        const double2 rwv = __ldcg(rwb + r * BN + c);
-        sh.srv.a3[r][c] = c < jn ? rwv : cmk(0.0, 0.0);
+      constexpr int kPer = kPB * kPB / kServerThreads;
+      double2 v1[kPer], v2[kPer], v3[kPer];
+#pragma unroll
+      for (int u = 0; u < kPer; u++) {  // all loads in flight before the first use
+        const int e = t + u * kServerThreads, r = e / kPB, c = e % kPB;
+        v1[u] = __ldcg(sb + e);
+        v2[u] = __ldcg(pcb + r * kPB + (c ^ ((r & 1) << 2)));
+        v3[u] = __ldcg(rwb + r * BN + c);
+      }
+#pragma unroll
+      for (int u = 0; u < kPer; u++) {
+        const int e = t + u * kServerThreads, r = e / kPB, c = e % kPB;
+        sh.srv.a1[r][c] = v1[u];
+        sh.srv.a2[r][c] = r < jn ? cneg(v2[u]) : cmk(0.0, 0.0);
+        sh.srv.a3[r][c] = c < jn ? v3[u] : cmk(0.0, 0.0);
       }
     }
     if (t < kPB) sh.perm[t] = t;
@@ -911,7 +919,6 @@ __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, 
     }
     bar_sync(kBarMath, kServerThreads);
     if (t == 0) {
-      __threadfence();
       st_release(sy.t_flag, s);
       trace_ev(p, s, kTrPanelTout);
     }

@@ -48,7 +48,9 @@ enum { kTrMathStart = 0, kTrMathOperands, kTrMathCopied, kTrMathPublished, kTrMa
        // finer grain: server pieces loaded / next pivot block formed / GJ done
        kTrSrvLoaded, kTrSrvSchur, kTrSrvGJ,
        // publication of the pivot rows / columns and of the server blocks (lead warp)
-       kTrGlobEnter, kTrGlobStored, kTrSrvPubEnter, kTrSrvPubStored, kTrSrvPubDone, kTraceEvents };
+       kTrGlobEnter, kTrGlobStored, kTrSrvPubEnter, kTrSrvPubStored, kTrSrvPubDone,
+       // T-server: end of the factorization of each 4-pivot group
+       kTrSrvGroup0, kTraceEvents = kTrSrvGroup0 + 8 };
 
 inline int persist_flag_words(int TR, int TC) { return TR + TC + 1 + TR * TC + 1 + 2 + 1; }
 inline int persist_cons_words(int TR, int TC) { return 2 * TR + 2 * TC + 2 + 2 * TC + 2; }
