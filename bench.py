@@ -204,11 +204,12 @@ def measure_fp64_peak(device: int):
     return FP64_DMMA_FALLBACK_TFLOPS, "fallback: earlier FP64 DMMA measurement on this pool (37 TFLOP/s)"
 
 
-def grad_over_fwd(h, dev, stream, reps: int = 3):
+def grad_over_fwd(h, dev, stream, reps: int = 5):
     """Config-5 adjoint cost: time of rgf_smatrix_grad_2d (S and dF/d eps for
     F = sum |t_ab|^2 over 8 left inputs -> 8 right outputs, checkpoint every 23
     slices) over the time of the forward rgf_smatrix_2d, both device-resident
-    and timed with CUDA events on the library's stream."""
+    and timed with CUDA events on the library's stream (median of 5 calls
+    after 3 warm-up calls)."""
     import torch
 
     from rgf_b200 import _abi, workloads
@@ -234,22 +235,47 @@ def grad_over_fwd(h, dev, stream, reps: int = 3):
                                            D.data_ptr(), 8, S.data_ptr(), 8, g.data_ptr(), 23))
 
     def t(fn):
-        for _ in range(2):
+        for _ in range(3):
             fn()
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
+        ts = []
         for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
             fn()
-        e1.record(stream)
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / reps
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
 
     tf = t(fwd)
     tg = t(grad)
     return {"value": tg / tf, "fwd_ms": tf, "grad_ms": tg,
             "workload": "config5: 2D periodic N=256, L=512, eps 1+3U, k0dx=2pi/15, t = S(out R 1:8, in L 1:8), "
                         "F = sum|t|^2, checkpoint every 23 slices"}
+
+
+def batch_rate(dev, count: int = 32, workers: int = 8):
+    """Config-4 batched form: the first `count` of the 256 seeded structures
+    (N uniform 64..512, L uniform 100..2000, eps 1+2U, complex k0dx), full S
+    each, through rgf_smatrix_batch_2d with host inputs and outputs; timed by
+    the host around the blocking call (warm-up call first)."""
+    import rgf_b200
+    from rgf_b200 import workloads
+    items = [workloads.config4_structure(k) for k in range(count)]
+    systs = [it[0] for it in items]
+    outs = [it[1] for it in items]
+    ins = [it[2] for it in items]
+    rgf_b200.cal_smatrix_RGF_batch(systs[:4], outs[:4], ins[:4], workers=workers, device=dev)
+    t0 = time.perf_counter()
+    rgf_b200.cal_smatrix_RGF_batch(systs, outs, ins, workers=workers, device=dev)
+    dt = time.perf_counter() - t0
+    Ns, Ls, _ = workloads.config4_params()
+    return {"value": count / dt, "unit": "S-matrices/s", "structures": count, "workers": workers,
+            "seconds": dt, "sum_L_N3": float(np.sum(Ls[:count].astype(float) * Ns[:count].astype(float) ** 3)),
+            "workload": "config4: first structures of the 256-structure batch (N U{64..512}, L U{100..2000}, "
+                        "eps 1+2U, k0dx = 2pi/15 (1 + i eta), eta U[0,1e-3), periodic, full S)",
+            "timing": "host wall clock around the blocking batch call; inputs and S on the host"}
 
 
 def config_dict():
@@ -353,6 +379,7 @@ def run_ours(args, dist):
     line["canonical_tflops"] = F * value / 1e12 / dist.world
     line["precision_form"] = None
     line["grad_over_fwd"] = grad_over_fwd(h, dev, stream) if not args.slices else None
+    line["batch"] = batch_rate(dev) if not args.slices else None
     n, ms, fl_exec, name = prof
     fl = nx * workloads.canonical_slice_flops(ny, n_in // 2, n_out // 2)  # the launch covers all nx slices
     achieved = fl / (ms / n / 1e3) / 1e12 if n else None

@@ -149,6 +149,19 @@ RGF_API rgf_status rgf_smatrix_2d(rgf_handle h, const rgf_syst2d* syst, const rg
 RGF_API rgf_status rgf_smatrix_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_request* req,
                           const rgf_options* opt, rgf_cplx* S, int64_t ldS, rgf_channels* ch);
 
+/* Batched form: `count` independent 2D problems (each as rgf_smatrix_2d:
+ * systs[i], reqs[i], S[i] with leading dimension ldS[i]; all host or all
+ * device per opt->S_on_device), run as `workers` concurrent pipelines (<= 0:
+ * 8), each with its own stream and workspace inside the handle, largest
+ * problems first.  The pipelines' persistent sweeps share the GPU's SMs
+ * through one budget, so their cooperative grids are always co-resident.
+ * statuses (may be NULL) receives each problem's status; the return value
+ * is the first failure (message names the item).  The reference has no
+ * batched call: its user loops over cal_smatrix_RGF. */
+RGF_API rgf_status rgf_smatrix_batch_2d(rgf_handle h, int64_t count, const rgf_syst2d* systs,
+                                        const rgf_request* reqs, const rgf_options* opt, rgf_cplx* const* S,
+                                        const int64_t* ldS, rgf_status* statuses, int32_t workers);
+
 /* Permittivity gradient (an addition: the reference computes S only).
  * Computes S as rgf_smatrix_2d/3d and
  *     g[m + n*N] = sum_ab D[a + b*ldD] * dS_ab / d epsilon[m, n]

@@ -70,6 +70,8 @@ SIGNATURES = {
                                POINTER(Channels)]),
     "rgf_smatrix_3d": (c_int, [c_void_p, POINTER(Syst3D), POINTER(Request), POINTER(Options), c_void_p, c_int64,
                                POINTER(Channels)]),
+    "rgf_smatrix_batch_2d": (c_int, [c_void_p, c_int64, POINTER(Syst2D), POINTER(Request), POINTER(Options),
+                                     POINTER(c_void_p), POINTER(c_int64), POINTER(c_int), c_int32]),
     "rgf_smatrix_grad_2d": (c_int, [c_void_p, POINTER(Syst2D), POINTER(Request), POINTER(Options), c_void_p,
                                     c_int64, c_void_p, c_int64, c_void_p, c_int64]),
     "rgf_smatrix_grad_3d": (c_int, [c_void_p, POINTER(Syst3D), POINTER(Request), POINTER(Options), c_void_p,

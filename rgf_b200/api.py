@@ -282,6 +282,45 @@ def cal_smatrix_RGF_3D(syst, out, in_, *, device: int = 0, options=None, handle=
     return S, _channels_dict_3d(cb, nx, ny, bc)
 
 
+def cal_smatrix_RGF_batch(systs, outs, ins, *, workers: int = 0, device: int = 0, options=None, handle=None):
+    """[S_1, ..., S_n] for n independent 2D structures (cal_smatrix_RGF on
+    each), computed as concurrent pipelines on the GPU; outs / ins are lists
+    (one request per structure) or a single request used for all."""
+    n = len(systs)
+    if not isinstance(outs, (list, tuple)) or (outs and isinstance(outs[0], str)):
+        outs = [outs] * n
+    if not isinstance(ins, (list, tuple)) or (ins and isinstance(ins[0], str)):
+        ins = [ins] * n
+    h = handle or _abi.default_handle(device)
+    keep, sy_list, rq_list, S_list = [], [], [], []
+    for syst, out, in_ in zip(systs, outs, ins):
+        _check_syst(syst, "yBC")
+        eps = np.asarray(_get(syst, "epsilon"))
+        ny, nx = eps.shape
+        bc, ka = _bc_2d(_get(syst, "yBC"))
+        req, k = _request(out, in_)
+        epsf = np.ascontiguousarray(eps.astype(complex).ravel(order="F"))
+        sy = Syst2D(ny, nx, ptr(epsf), 0, cplx(_get(syst, "epsilon_L")), cplx(_get(syst, "epsilon_R")),
+                    cplx(_get(syst, "k0dx")), bc, ka)
+        no, ni = ctypes.c_int64(), ctypes.c_int64()
+        check(h.lib.rgf_smatrix_size_2d(h.h, ctypes.byref(sy), ctypes.byref(req), ctypes.byref(no),
+                                        ctypes.byref(ni)))
+        S = np.zeros((max(no.value, 1), max(ni.value, 1)), dtype=complex, order="F")
+        keep += [k, epsf]
+        sy_list.append(sy)
+        rq_list.append(req)
+        S_list.append((S, no.value, ni.value))
+    systs_c = (Syst2D * n)(*sy_list)
+    reqs_c = (Request * n)(*rq_list)
+    Sp = (ctypes.c_void_p * n)(*[S.ctypes.data for S, _, _ in S_list])
+    ld = (ctypes.c_int64 * n)(*[S.shape[0] for S, _, _ in S_list])
+    stat = (ctypes.c_int * n)()
+    opt = _options(options)
+    check(h.lib.rgf_smatrix_batch_2d(h.h, n, systs_c, reqs_c, ctypes.byref(opt), Sp, ld, stat, int(workers)))
+    del keep
+    return [S[:no, :ni] if (no and ni) else np.zeros((no, ni)) for S, no, ni in S_list]
+
+
 def smatrix_grad_RGF(syst, out, in_, D, *, checkpoint: int = 0, device: int = 0, options=None, handle=None):
     """(S, g) for a 2D syst: S as cal_smatrix_RGF, and
     g[m, n] = sum_ab D[a, b] dS_ab / d epsilon[m, n] (complex, shape [ny, nx]).

@@ -960,10 +960,19 @@ int persist_threads(int BM, int BN) {
 }
 
 // tile shape: the largest that keeps >= 60% of the SMs busy, else the one
-// with the most CTAs; one SM always stays free for the T-server CTA
-bool persist_choose_tile(int64_t R, int64_t C, int sms, int* BM, int* BN) {
+// with the most CTAs; one SM always stays free for the T-server CTA.  With
+// prefer_large (several sweeps sharing the GPU) simply the largest tile whose
+// grid fits in `sms`.
+bool persist_choose_tile(int64_t R, int64_t C, int sms, int* BM, int* BN, bool prefer_large) {
   const int cand[3] = {96, 64, 32};
   const int avail = sms - 1;
+  for (int q = 0; q < 3 && prefer_large; q++) {
+    const int64_t tiles = ((R + cand[q] - 1) / cand[q]) * ((C + cand[q] - 1) / cand[q]);
+    if (tiles <= avail) {
+      *BM = *BN = cand[q];
+      return true;
+    }
+  }
   for (int q = 0; q < 3; q++) {
     const int64_t tiles = ((R + cand[q] - 1) / cand[q]) * ((C + cand[q] - 1) / cand[q]);
     if (tiles <= avail && tiles * 10 >= (int64_t)avail * 6) {

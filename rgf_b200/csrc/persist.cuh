@@ -57,7 +57,7 @@ inline int persist_cons_words(int TR, int TC) { return 2 * TR + 2 * TC + 2 + 2 *
 
 size_t persist_smem_bytes();
 int persist_threads(int BM, int BN);
-bool persist_choose_tile(int64_t R, int64_t C, int sms, int* BM, int* BN);
+bool persist_choose_tile(int64_t R, int64_t C, int sms, int* BM, int* BN, bool prefer_large = false);
 cudaError_t launch_persist(const PersistParams& p, int BM, int BN, cudaStream_t s);
 
 }  // namespace rgf

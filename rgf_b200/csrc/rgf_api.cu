@@ -14,6 +14,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <string>
 #include <chrono>
 #include <mutex>
@@ -61,6 +62,11 @@ struct rgf_handle_s {
   DevBuf xpc, xrow, xt, xu, xsync, xprobe, xtrace;  // persistent-kernel exchange buffers
   DevBuf gck, gseg, gm0, gpsi, gphi, get, gd, gg;   // permittivity gradient (checkpoints, carriers)
   int sms = 0;
+  // batched calls: one sub-handle per concurrent pipeline (own stream and
+  // workspace, a share of the SMs for its persistent sweeps)
+  std::vector<rgf_handle_s*> workers;
+  std::atomic<int> sm_free{0};          // batch parent: SMs not held by a running sweep
+  std::atomic<int>* sm_budget = nullptr;  // batch worker: the parent's counter
   int64_t launches = 0;
   std::string prof_kernel;
   double probe = 0.0;
@@ -568,7 +574,8 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
     return RGF_OK;
   };
   int BMp = 0, BNp = 0;
-  bool use_persist = L > 0 && !(opt && opt->engine == 1) && persist_choose_tile(Rp, Cp, h->sms, &BMp, &BNp);
+  bool use_persist = L > 0 && !(opt && opt->engine == 1) &&
+                     persist_choose_tile(Rp, Cp, h->sms, &BMp, &BNp, h->sm_budget != nullptr);
   unsigned long long* probe_d = nullptr;
   h->prof_kernel = sweep_update_kernel_name();
   if (use_persist) {
@@ -657,7 +664,22 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
         }
         RGF_CUDA_TRY(cudaEventRecord(h->ev[ev_used], h->stream));
       }
+      // in a batch, hold SMs for the whole cooperative grid while it runs, so
+      // that the grids of concurrent pipelines always fit on the GPU together
+      const int need = TR * TC + 1;
+      if (h->sm_budget) {
+        for (;;) {
+          int cur = h->sm_budget->load();
+          if (cur >= need && h->sm_budget->compare_exchange_weak(cur, cur - need)) break;
+          std::this_thread::sleep_for(std::chrono::microseconds(20));
+        }
+      }
       cudaError_t e = launch_persist(pp, BMp, BNp, h->stream);
+      if (h->sm_budget) {
+        const cudaError_t se = cudaStreamSynchronize(h->stream);
+        h->sm_budget->fetch_add(need);
+        RGF_CUDA_TRY(se);
+      }
       if (e != cudaSuccess) {
         cudaGetLastError();
         use_persist = false;  // e.g. the cooperative launch does not fit: per-step engine below
@@ -737,9 +759,14 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
   };
   // gradient: checkpoints of the forward sweep (W after every K-th slice) and
   // the assembled first slice
-  const int64_t gK = gr ? (gr->checkpoint > 0 ? std::min<int64_t>(gr->checkpoint, std::max<int64_t>(L, 1))
-                                              : std::max<int64_t>(1, (int64_t)ceil(sqrt((double)L))))
-                        : 0;
+  // checkpoint interval: the caller's, else every slice when those snapshots
+  // take at most 2 GiB (no recomputation), else ceil(sqrt(L))
+  const int64_t gK =
+      !gr ? 0
+          : gr->checkpoint > 0 ? std::min<int64_t>(gr->checkpoint, std::max<int64_t>(L, 1))
+          : (double)L * Rp * ldm * sizeof(double2) <= 2.0 * (1 << 30)
+              ? 1
+              : std::max<int64_t>(1, (int64_t)ceil(sqrt((double)L)));
   if (gr && L > 0) {
     if ((st = ensure(h->gck, sizeof(double2) * Rp * ldm * std::max<int64_t>(1, L / gK)))) return st;
     if ((st = ensure(h->gm0, sizeof(double2) * Rp * ldm))) return st;
@@ -785,7 +812,7 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
     if ((st = ensure(h->gpsi, sizeof(double2) * 2 * N * nI))) return st;
     if ((st = ensure(h->gphi, sizeof(double2) * 2 * nO * N))) return st;
     if ((st = ensure(h->get, sizeof(double2) * nO * N))) return st;
-    if ((st = ensure(h->gseg, sizeof(double2) * gK * Rp * ldm))) return st;
+    if (gK > 1 && (st = ensure(h->gseg, sizeof(double2) * gK * Rp * ldm))) return st;
     if (!S_dev && (st = ensure(h->gg, sizeof(double2) * N * L))) return st;
     double2* Dd = as<double2>(h->gd);
     RGF_CUDA_TRY(cudaMemcpyAsync(Dd, Da.data(), sizeof(double2) * nO * nI, cudaMemcpyHostToDevice, h->stream));
@@ -805,27 +832,37 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
     const int64_t nseg = (L + gK - 1) / gK;
     for (int64_t sg = nseg - 1; sg >= 0; sg--) {
       const int64_t k_lo = sg * gK, k_hi = std::min(L, k_lo + gK);
-      if (sg == 0) {
-        RGF_CUDA_TRY(cudaMemcpyAsync(M, h->gm0.p, sizeof(double2) * Rp * ldm, cudaMemcpyDeviceToDevice, h->stream));
-      } else {
-        RGF_CUDA_TRY(cudaMemcpyAsync(M, as<double2>(h->gck) + (sg - 1) * Rp * ldm, sizeof(double2) * Rp * ldm,
-                                     cudaMemcpyDeviceToDevice, h->stream));
-        launch_assemble(M, ldm, N, N + no_s, M, ldm, nullptr, 0, st_col, st_val, k2, slice_eps(k_lo), cmk(0, 0),
-                        h->stream);
-        h->launches++;
+      // with a snapshot of every slice (gK == 1) nothing is recomputed
+      const double2* segW = gK == 1 ? as<double2>(h->gck) + k_lo * Rp * ldm : seg;
+      if (gK > 1) {
+        if (sg == 0) {
+          RGF_CUDA_TRY(
+              cudaMemcpyAsync(M, h->gm0.p, sizeof(double2) * Rp * ldm, cudaMemcpyDeviceToDevice, h->stream));
+        } else {
+          RGF_CUDA_TRY(cudaMemcpyAsync(M, as<double2>(h->gck) + (sg - 1) * Rp * ldm, sizeof(double2) * Rp * ldm,
+                                       cudaMemcpyDeviceToDevice, h->stream));
+          launch_assemble(M, ldm, N, N + no_s, M, ldm, nullptr, 0, st_col, st_val, k2, slice_eps(k_lo), cmk(0, 0),
+                          h->stream);
+          h->launches++;
+        }
+        if ((st = run_slices(k_lo, k_hi, seg, 1))) return st;
       }
-      if ((st = run_slices(k_lo, k_hi, seg, 1))) return st;
       for (int64_t j = k_hi - 1; j >= k_lo; j--) {
-        const double2* Wj = seg + (j - k_lo) * Rp * ldm;
+        const double2* Wj = segW + (j - k_lo) * Rp * ldm;
         const int nx_ = cur ^ 1;
-        launch_copy_pad(psi[nx_], nI, N, nI, Wj + N, ldm, N, ni_s, h->stream);
-        launch_zgemm(N, nI, N, one, ZOp{Wj, ldm, 0}, ZOp{psi[cur], nI, 0}, one, psi[nx_], nI, h->stream);
-        launch_copy_pad(phv[nx_], N, nO, N, Wj + N * ldm, ldm, no_s, N, h->stream);
-        launch_zgemm(nO, N, N, one, ZOp{phv[cur], N, 0}, ZOp{Wj, ldm, 0}, one, phv[nx_], N, h->stream);
-        launch_zgemm(nO, N, nI, one, ZOp{Dd, nI, 0}, ZOp{psi[nx_], nI, 1}, zero, Et, N, h->stream);
+        launch_zgemm_add(N, nI, N, ZOp{Wj, ldm, 0}, ZOp{psi[cur], nI, 0}, ZAdd{Wj + N, ldm, N, ni_s}, psi[nx_],
+                         nI, h->stream);
+        launch_zgemm_add(nO, N, N, ZOp{phv[cur], N, 0}, ZOp{Wj, ldm, 0}, ZAdd{Wj + N * ldm, ldm, no_s, N},
+                         phv[nx_], N, h->stream);
         const int64_t n_phys = mirror ? L - 1 - j : j;
-        launch_grad_slice(phv[nx_], Et, N, nO, coef, gout + n_phys * N, h->stream);
-        h->launches += 6;
+        if (nO * nI <= 1024) {
+          launch_grad_fused(phv[nx_], psi[nx_], Dd, N, (int)nO, (int)nI, coef, gout + n_phys * N, h->stream);
+          h->launches += 3;
+        } else {
+          launch_zgemm(nO, N, nI, one, ZOp{Dd, nI, 0}, ZOp{psi[nx_], nI, 1}, zero, Et, N, h->stream);
+          launch_grad_slice(phv[nx_], Et, N, nO, coef, gout + n_phys * N, h->stream);
+          h->launches += 4;
+        }
         cur = nx_;
       }
       if ((st = check_launch())) return st;
@@ -997,6 +1034,7 @@ rgf_status rgf_destroy(rgf_handle h) {
     if (b->p) cudaFree(b->p);
   for (cudaEvent_t ev : h->ev) cudaEventDestroy(ev);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  for (rgf_handle_s* w : h->workers) rgf_destroy(w);
   delete h;
   return RGF_OK;
 }
@@ -1021,6 +1059,75 @@ rgf_status rgf_smatrix_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_reques
     return RGF_ERR_ARG;
   }
   return smatrix(h, problem3d(syst), req, opt, S, ldS, ch);
+}
+
+rgf_status rgf_smatrix_batch_2d(rgf_handle h, int64_t count, const rgf_syst2d* systs, const rgf_request* reqs,
+                                const rgf_options* opt, rgf_cplx* const* S, const int64_t* ldS,
+                                rgf_status* statuses, int32_t workers) {
+  rgf_status st;
+  if ((st = check_handle(h))) return st;
+  if (count < 0 || (count > 0 && (!systs || !reqs || !S || !ldS))) {
+    set_error("batch: count must be >= 0 and systs, reqs, S, ldS non-NULL");
+    return RGF_ERR_ARG;
+  }
+  if (count == 0) return RGF_OK;
+  if (opt && opt->profile > 0) {
+    set_error("batch: profiling is per call; use rgf_smatrix_2d");
+    return RGF_ERR_ARG;
+  }
+  int nw = workers > 0 ? workers : 8;
+  nw = (int)std::min<int64_t>(nw, count);
+  nw = std::max(1, std::min(nw, h->sms / 2));
+  RGF_CUDA_TRY(cudaSetDevice(h->device));
+  while ((int)h->workers.size() < nw) {
+    rgf_handle w = nullptr;
+    if ((st = rgf_create(h->device, &w))) return st;
+    h->workers.push_back(w);
+  }
+  // the pipelines' persistent sweeps draw their SMs from one budget (a sweep
+  // waits until its whole grid fits), so their cooperative grids are always
+  // co-resident; each picks the largest tile whose grid fits the GPU
+  h->sm_free.store(h->sms);
+  for (int i = 0; i < nw; i++) {
+    h->workers[i]->sms = h->sms;
+    h->workers[i]->sm_budget = &h->sm_free;
+  }
+  // largest first (sum over slices of N^3 + N^2 P), so that the pipelines finish together
+  std::vector<int64_t> order(count);
+  for (int64_t i = 0; i < count; i++) order[i] = i;
+  std::vector<double> cost(count);
+  for (int64_t i = 0; i < count; i++) {
+    const double N = (double)systs[i].ny;
+    cost[i] = (double)std::max<int64_t>(systs[i].nx, 1) * N * N * N;
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return cost[a] > cost[b]; });
+  std::vector<rgf_status> res(count, RGF_OK);
+  std::vector<std::string> msg(count);
+  std::atomic<int64_t> next(0);
+  auto work = [&](int wi) {
+    rgf_handle w = h->workers[wi];
+    cudaSetDevice(w->device);
+    for (;;) {
+      const int64_t k = next.fetch_add(1);
+      if (k >= count) break;
+      const int64_t i = order[k];
+      res[i] = smatrix(w, problem2d(&systs[i]), &reqs[i], opt, S[i], ldS[i], nullptr);
+      if (res[i] != RGF_OK) msg[i] = tl_err;
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int i = 1; i < nw; i++) pool.emplace_back(work, i);
+  work(0);
+  for (auto& th : pool) th.join();
+  rgf_status first = RGF_OK;
+  for (int64_t i = 0; i < count; i++) {
+    if (statuses) statuses[i] = res[i];
+    if (res[i] != RGF_OK && first == RGF_OK) {
+      first = res[i];
+      set_error("batch item " + std::to_string(i) + ": " + msg[i]);
+    }
+  }
+  return first;
 }
 
 rgf_status rgf_smatrix_grad_2d(rgf_handle h, const rgf_syst2d* syst, const rgf_request* req,

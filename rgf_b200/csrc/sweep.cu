@@ -50,7 +50,7 @@ constexpr size_t kGemmSmem = sizeof(double2) * (kBM * kAS + kBK * kBS);
 template <bool kMask>
 __global__ void __launch_bounds__(128) k_zgemm(int64_t M, int64_t N, int64_t K, double2 alpha, ZOp A,
                                                ZOp B, double2 beta, double2* C, int64_t ldc,
-                                               int64_t j0, int64_t jn) {
+                                               int64_t j0, int64_t jn, ZAdd add) {
   extern __shared__ double2 smem[];
   double2* As = smem;               // [kBM][kAS]
   double2* Bs = smem + kBM * kAS;   // [kBK][kBS]
@@ -120,22 +120,35 @@ __global__ void __launch_bounds__(128) k_zgemm(int64_t M, int64_t N, int64_t K, 
           const bool masked = kMask && (rmask || (c >= j0 && c < j0 + jn));
           if (!masked) v = cadd(v, cmul(beta, C[r * ldc + c]));
         }
+        if (add.p && r < add.rows && c < add.cols) v = cadd(v, add.p[r * add.ld + c]);
         C[r * ldc + c] = v;
       }
     }
   }
 }
 
-void launch_zgemm(int64_t M, int64_t N, int64_t K, double2 alpha, ZOp A, ZOp B, double2 beta,
-                  double2* C, int64_t ldc, cudaStream_t s) {
+static void zgemm_attr() {
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_zgemm<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
     cudaFuncSetAttribute(k_zgemm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem);
     attr = true;
   }
+}
+
+void launch_zgemm(int64_t M, int64_t N, int64_t K, double2 alpha, ZOp A, ZOp B, double2 beta,
+                  double2* C, int64_t ldc, cudaStream_t s) {
+  zgemm_attr();
   dim3 grid((unsigned)((N + kBN - 1) / kBN), (unsigned)((M + kBM - 1) / kBM));
-  k_zgemm<false><<<grid, 128, kGemmSmem, s>>>(M, N, K, alpha, A, B, beta, C, ldc, 0, 0);
+  k_zgemm<false><<<grid, 128, kGemmSmem, s>>>(M, N, K, alpha, A, B, beta, C, ldc, 0, 0, ZAdd{nullptr, 0, 0, 0});
+}
+
+// C = A B + add (add read in its rows x cols corner, zero elsewhere)
+void launch_zgemm_add(int64_t M, int64_t N, int64_t K, ZOp A, ZOp B, ZAdd add, double2* C, int64_t ldc,
+                      cudaStream_t s) {
+  zgemm_attr();
+  dim3 grid((unsigned)((N + kBN - 1) / kBN), (unsigned)((M + kBM - 1) / kBM));
+  k_zgemm<false><<<grid, 128, kGemmSmem, s>>>(M, N, K, cmk(1.0, 0.0), A, B, cmk(0.0, 0.0), C, ldc, 0, 0, add);
 }
 
 // ---------------------------------------------------------------------------
@@ -266,7 +279,8 @@ void launch_sweep_update(double2* M, int64_t ldm, int64_t R, int64_t Cc, int64_t
   }
   ZOp A{Pc, kSw, 0}, B{U, ldu, 0};
   dim3 grid((unsigned)((Cc + kBN - 1) / kBN), (unsigned)((R + kBM - 1) / kBM));
-  k_zgemm<true><<<grid, 128, kGemmSmem, s>>>(R, Cc, kSw, cmk(-1.0, 0.0), A, B, cmk(1.0, 0.0), M, ldm, j0, jn);
+  k_zgemm<true><<<grid, 128, kGemmSmem, s>>>(R, Cc, kSw, cmk(-1.0, 0.0), A, B, cmk(1.0, 0.0), M, ldm, j0, jn,
+                                             ZAdd{nullptr, 0, 0, 0});
 }
 
 const char* sweep_update_kernel_name() { return "k_zgemm<true> (sweep rank-32 update, FP64 DMMA)"; }
@@ -481,21 +495,29 @@ void launch_scale_cols(const double2* src, int64_t lds, const double2* diag, dou
 // ---------------------------------------------------------------------------
 // permittivity gradient
 // ---------------------------------------------------------------------------
-// dst (rows x cols, row-major, ld ldd) = src in its top-left src_rows x
-// src_cols corner, zero elsewhere
-__global__ void k_copy_pad(double2* dst, int64_t ldd, int64_t rows, int64_t cols, const double2* src, int64_t lds,
-                           int64_t src_rows, int64_t src_cols) {
-  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (c >= cols) return;
-  for (int64_t r = blockIdx.y; r < rows; r += gridDim.y)
-    dst[r * ldd + c] = (r < src_rows && c < src_cols) ? src[r * lds + c] : cmk(0.0, 0.0);
+// g[m] = coef * sum_a Phi[a][m] sum_b D[a][b] Psi[m][b]  (Phi: n_out x N, Psi:
+// N x n_in, D: n_out x n_in, all row-major), for small n_out * n_in (D staged
+// in shared memory)
+__global__ void k_grad_fused(const double2* Phi, const double2* Psi, const double2* D, int64_t N, int n_out,
+                             int n_in, double2 coef, double2* g) {
+  extern __shared__ double2 Ds[];
+  for (int e = threadIdx.x; e < n_out * n_in; e += blockDim.x) Ds[e] = D[e];
+  __syncthreads();
+  const int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (m >= N) return;
+  double2 acc = cmk(0.0, 0.0);
+  for (int a = 0; a < n_out; a++) {
+    double2 e = cmk(0.0, 0.0);
+    for (int b = 0; b < n_in; b++) e = cadd(e, cmul(Ds[a * n_in + b], Psi[m * n_in + b]));
+    acc = cadd(acc, cmul(Phi[a * N + m], e));
+  }
+  g[m] = cmul(coef, acc);
 }
 
-void launch_copy_pad(double2* dst, int64_t ldd, int64_t rows, int64_t cols, const double2* src, int64_t lds,
-                     int64_t src_rows, int64_t src_cols, cudaStream_t s) {
-  if (rows <= 0 || cols <= 0) return;
-  dim3 grid((unsigned)((cols + 127) / 128), (unsigned)(rows < 4096 ? rows : 4096));
-  k_copy_pad<<<grid, 128, 0, s>>>(dst, ldd, rows, cols, src, lds, src_rows, src_cols);
+void launch_grad_fused(const double2* Phi, const double2* Psi, const double2* D, int64_t N, int n_out, int n_in,
+                       double2 coef, double2* g, cudaStream_t s) {
+  k_grad_fused<<<(unsigned)((N + 127) / 128), 128, sizeof(double2) * n_out * n_in, s>>>(Phi, Psi, D, N, n_out,
+                                                                                        n_in, coef, g);
 }
 
 // g[m] = coef * sum_a Phi[a][m] Et[a][m]  (Phi, Et: n_out x N row-major)

@@ -12,8 +12,16 @@ struct ZOp {
   int op;
 };
 
+// addend of a GEMM: C = A B + add, add read in its rows x cols corner (row-major, ld)
+struct ZAdd {
+  const double2* p;
+  int64_t ld, rows, cols;
+};
+
 void launch_zgemm(int64_t M, int64_t N, int64_t K, double2 alpha, ZOp A, ZOp B, double2 beta, double2* C,
                   int64_t ldc, cudaStream_t s);
+void launch_zgemm_add(int64_t M, int64_t N, int64_t K, ZOp A, ZOp B, ZAdd add, double2* C, int64_t ldc,
+                      cudaStream_t s);
 int sweep_block_width();
 void launch_sweep_panel(const double2* M, int64_t ldm, int64_t R, int64_t Cc, int64_t j0, int jn, double2* Pc,
                         double2* U, int64_t ldu, int* status, cudaStream_t s);
@@ -35,10 +43,11 @@ void launch_probe_init(double2* M, int64_t ldm, int64_t N, int64_t R, int64_t pc
 void launch_check_finite(const double2* x, int64_t n, int* status, cudaStream_t s);
 void launch_scale_cols(const double2* src, int64_t lds, const double2* diag, double2* dst, int64_t ldd,
                        int64_t rows, int64_t cols, cudaStream_t s);
-// permittivity gradient: zero-padded copy and the per-slice contraction
-// g[m] = coef * sum_a Phi[a][m] Et[a][m]
-void launch_copy_pad(double2* dst, int64_t ldd, int64_t rows, int64_t cols, const double2* src, int64_t lds,
-                     int64_t src_rows, int64_t src_cols, cudaStream_t s);
+// permittivity gradient: the per-slice contraction
+// g[m] = coef * sum_a Phi[a][m] sum_b D[a][b] Psi[m][b] (fused for small D, else
+// through Et = D Psi^T)
+void launch_grad_fused(const double2* Phi, const double2* Psi, const double2* D, int64_t N, int n_out, int n_in,
+                       double2 coef, double2* g, cudaStream_t s);
 void launch_grad_slice(const double2* Phi, const double2* Et, int64_t N, int64_t n_out, double2 coef, double2* g,
                        cudaStream_t s);
 
