@@ -57,19 +57,26 @@ def log(*a):
 # distributed plumbing (replicas only)
 # ---------------------------------------------------------------------------
 class Dist:
-    def __init__(self):
+    """One process per GPU (torchrun environment); NCCL on GPUs, gloo on the
+    CPU (tests).  The path has no collective: the group only carries the
+    barriers around the timed region and the max of the ranks' times."""
+
+    def __init__(self, backend: str = "nccl", timeout_s: float = 300.0):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
         self.pg = None
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local_rank)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(minutes=20),
-                                    device_id=torch.device("cuda", self.local_rank))
+            kw = {}
+            if backend == "nccl":
+                torch.cuda.set_device(self.local_rank)
+                kw["device_id"] = torch.device("cuda", self.local_rank)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s), **kw)
             self.pg = dist
 
     def barrier(self):
@@ -80,13 +87,19 @@ class Dist:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        t = torch.tensor([x], dtype=torch.float64, device="cuda" if self.backend == "nccl" else "cpu")
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
     def close(self):
         if self.pg:
             self.pg.destroy_process_group()
+
+
+def whole_job_rate(steps: int, world: int, max_ms: float) -> float:
+    """S-matrices/s of the whole job: every rank computes `steps` S-matrices
+    (replicas), timed as the max over ranks of the device time."""
+    return steps * world / (max_ms / 1e3)
 
 
 # ---------------------------------------------------------------------------
@@ -364,8 +377,8 @@ def run_ours(args, dist):
     e_ms, _ = timed(False, args.steps, 0)
     dist.barrier()
     e_ms = dist.max(e_ms)
-    value = args.steps * dist.world / (t_ms / 1e3)
-    e2e = args.steps * dist.world / (e_ms / 1e3)
+    value = whole_job_rate(args.steps, dist.world, t_ms)
+    e2e = whole_job_rate(args.steps, dist.world, e_ms)
 
     S = S_dev.cpu().numpy().T  # n_out x n_in
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
