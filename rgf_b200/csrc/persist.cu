@@ -672,16 +672,28 @@ __device__ void panel_role(const PersistParams& p, Shared& sh, const Sync& sy, i
     bar_sync(kBarPanel, kPanelThreads);
     if (sh.panel_abort) return;
     const double2* tb = p.tbuf + (size_t)par * kPB * kPB;
-    for (int e = t; e < kPB * kPB; e += kPanelThreads) sh.T[e / kPB][e % kPB] = __ldcg(tb + e);
     const double2* rows = p.rowbuf + ((size_t)par * p.TC + Cq) * (kPB * BN);
     double2* ub = p.ubuf + ((size_t)par * p.TC + Cq) * (kPB * BN);
+    constexpr int kPer = kPB * kPB / kPanelThreads;
     bool waited_u = false;
     for (int cc = 0; cc < w; cc += kPB) {
       const int wc = min(kPB, w - cc);
-      for (int e = t; e < kPB * kPB; e += kPanelThreads) {
-        const int q = e / kPB, c = e % kPB;
-        sh.Mr[q][c] = (c < wc) ? __ldcg(rows + q * BN + cs + cc + c) : cmk(0.0, 0.0);
+      // the loads of T (first chunk) and of this chunk of pivot rows, each
+      // batch in flight at once
+      double2 v[kPer];
+      if (cc == 0) {
+#pragma unroll
+        for (int u = 0; u < kPer; u++) v[u] = __ldcg(tb + t + u * kPanelThreads);
+#pragma unroll
+        for (int u = 0; u < kPer; u++) sh.T[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
       }
+#pragma unroll
+      for (int u = 0; u < kPer; u++) {
+        const int e = t + u * kPanelThreads, q = e / kPB, c = e % kPB;
+        v[u] = (c < wc) ? __ldcg(rows + q * BN + cs + cc + c) : cmk(0.0, 0.0);
+      }
+#pragma unroll
+      for (int u = 0; u < kPer; u++) sh.Mr[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
       bar_sync(kBarPanel, kPanelThreads);
       if (!waited_u) {
         if (t == 0) sh.panel_abort = (s >= 2) ? !wait_ge(p, sy.u_cons + par * p.TC + Cq, p.TR * (s >> 1)) : 0;
@@ -861,7 +873,12 @@ __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, 
     bar_sync(kBarMath, kServerThreads);
     if (sh.panel_abort) return;
     if (k == 0) {
-      for (int e = t; e < kPB * kPB; e += kServerThreads) sh.srv.a1[e / kPB][e % kPB] = __ldcg(p.djjbuf + e);
+      constexpr int kPer = kPB * kPB / kServerThreads;
+      double2 v1[kPer];
+#pragma unroll
+      for (int u = 0; u < kPer; u++) v1[u] = __ldcg(p.djjbuf + t + u * kServerThreads);
+#pragma unroll
+      for (int u = 0; u < kPer; u++) sh.srv.a1[(t + u * kServerThreads) / kPB][(t + u * kServerThreads) % kPB] = v1[u];
     } else {
       const double2* sb = p.srvbuf + (size_t)par * kPB * kPB;
       const int w = k * kPB, parq = par ^ 1;
@@ -903,10 +920,12 @@ __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, 
 #pragma unroll
     for (int c = 0; c < 4; c++) a[c] = sh.srv.a1[lane][warp * 4 + c];
     gj_block<4>(p, sh, a, jn, t, kBarMath);
-    bar_sync(kBarMath, kServerThreads);
-    if (t == 0) trace_ev(p, s, kTrSrvGJ);
+    // perm is complete once the last pivot's barrier has passed
     if (t < kPB) sh.pinv[sh.perm[t]] = t;
-    if (t == 0) sh.panel_abort = (s >= 2) ? !wait_ge(p, sy.t_cons + par, ntiles * (s >> 1)) : 0;
+    if (t == 0) {
+      trace_ev(p, s, kTrSrvGJ);
+      sh.panel_abort = (s >= 2) ? !wait_ge(p, sy.t_cons + par, ntiles * (s >> 1)) : 0;
+    }
     bar_sync(kBarMath, kServerThreads);
     if (sh.panel_abort) return;
     double2* tb = p.tbuf + (size_t)par * kPB * kPB;
