@@ -46,7 +46,7 @@ METRIC = "S-matrices/s 2D N=1024 L=4096: 3xTF32+refine vs FP64 at 1e-10 rel err;
 UNIT = "S-matrices/s"
 FP64_DMMA_FALLBACK_TFLOPS = 37.0  # earlier measurement on this pool, used only if the live one fails
 PROFILE_EVERY = 64
-DRAM_BYTES_PER_SLICE = (20.993536e6 + 9.418240e6) / 16  # k_persist<96,96>, config 2, ncu over 16 slices
+DRAM_BYTES_PER_SLICE = (20.995072e6 + 8.149248e6) / 16  # k_persist<96,96>, config 2, ncu over 16 slices
 
 
 def log(*a):
