@@ -938,7 +938,7 @@ __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, 
     }
     bar_sync(kBarMath, kServerThreads);
     if (t == 0) {
-      st_release(sy.t_flag, s);
+      if (!p.withhold_t) st_release(sy.t_flag, s);
       trace_ev(p, s, kTrPanelTout);
     }
   }

@@ -35,6 +35,7 @@ struct PersistParams {
   int* abort;            // raised by the first wait that times out
   unsigned long long* probe_max;  // bits of max |G_n M_n v - v| (non-negative double)
   long long timeout_cycles;
+  int withhold_t;        // test hook: the T-server never releases its T flag
   // optional per-step event timestamps (%globaltimer, ns) for the first
   // trace_steps steps: trace[(cta * trace_steps + s) * kTraceEvents + e]
   unsigned long long* trace;

@@ -636,7 +636,14 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
       pp.probe_max = probe_d;
       int clk_khz = 2000000;
       cudaDeviceGetAttribute(&clk_khz, cudaDevAttrClockRate, h->device);
-      pp.timeout_cycles = (long long)clk_khz * 1000LL * 4;  // ~4 s per wait
+      // bound of every device-side wait: ~4 s, or RGF_WAIT_TIMEOUT_MS
+      const char* tmo_env = getenv("RGF_WAIT_TIMEOUT_MS");
+      const double tmo_ms = (tmo_env && atof(tmo_env) > 0) ? atof(tmo_env) : 4000.0;
+      pp.timeout_cycles = (long long)(clk_khz * tmo_ms);
+      // RGF_TEST_WITHHOLD_T=1 (failure-detection tests): the T-server never
+      // releases its T flag, so every dependent wait runs out
+      const char* wh_env = getenv("RGF_TEST_WITHHOLD_T");
+      pp.withhold_t = (wh_env && atoi(wh_env) == 1) ? 1 : 0;
       // RGF_TRACE=<file>: record per-step role timestamps of the first
       // RGF_TRACE_STEPS (default 128) steps of the first launch.
       // RGF_WATCH=<seconds> (with RGF_TRACE): if that launch is still running
@@ -892,13 +899,13 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
     set_error("syst.epsilon contains NaN or Inf");
     return RGF_ERR_NONFINITE;
   }
+  if (hstatus & kStatusTimeout) {  // before singular: what follows a timed-out sweep works on garbage
+    set_error("a device-side wait timed out");
+    return RGF_ERR_TIMEOUT;
+  }
   if (hstatus & kStatusSingular) {
     set_error("a pivot block of a slice matrix is singular");
     return RGF_ERR_SINGULAR;
-  }
-  if (hstatus & kStatusTimeout) {
-    set_error("a device-side wait timed out");
-    return RGF_ERR_TIMEOUT;
   }
   return copy_channels_out(h, tr, ci, ch);
 }
