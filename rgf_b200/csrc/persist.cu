@@ -88,6 +88,14 @@ __device__ __forceinline__ void st_release(int* p, int v) {
   asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ int ld_acquire_cta(const int* p) {
+  int v;
+  asm volatile("ld.acquire.cta.shared.s32 %0, [%1];" : "=r"(v) : "r"(smem_u32(p)) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_cta(int* p, int v) {
+  asm volatile("st.release.cta.shared.s32 [%0], %1;" ::"r"(smem_u32(p)), "r"(v) : "memory");
+}
 // volatile keeps predicated products from being if-converted into
 // unconditional ones; callers order the issue so that the two dependent
 // DMMAs of each complex product are far apart
@@ -102,17 +110,16 @@ __device__ __forceinline__ unsigned long long gtimer() {
   return t;
 }
 
-// 1/z = conj(z) / |z|^2 with the real reciprocal r = 1/n from the
-// single-precision approximation (rcp.approx) refined by two Newton-Raphson
-// steps r <- r + r (1 - n r) (quadratic convergence: ~23 -> ~46 -> full
-// double precision).  Branch-free: n is clamped to [1e-30, 1e30] so that
-// every lane of a warp can form it speculatively; pivots outside that range
-// are handled by the caller.
-__device__ __forceinline__ double2 crecip_fast(double2 z) {
-  const double n = fmin(fmax(z.x * z.x + z.y * z.y, 1e-30), 1e30);
-  float rf;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rf) : "f"((float)n));
-  double r = (double)rf;
+// 1/z = conj(z) r with r = 1/|z|^2 by the Newton-Raphson iteration for a
+// reciprocal, r <- r + r (1 - n r) (quadratic convergence), started from
+// rcp.approx.ftz.f64 and run twice: the result is within a few ulp of the
+// correctly rounded 1/n for every |z|^2 in the normal double range.
+// Branch-free, so every lane of a warp can form it speculatively; |z|^2 = 0
+// or subnormal gives a non-finite result, which the caller flags as singular.
+__device__ __forceinline__ double2 crecip_nr(double2 z) {
+  const double n = fma(z.x, z.x, z.y * z.y);
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(n));
   double e = fma(-n, r, 1.0);
   r = fma(r, e, r);
   e = fma(-n, r, 1.0);
@@ -143,9 +150,13 @@ struct Shared {
   int panel_abort;
   Blk T;   // panel role: T_s
   Blk Mr;  // panel role: my columns of the pivot rows
-  double2 fcol[2][kPB];   // T-server Gauss-Jordan: pivot column, reciprocal and row of a step
-  double2 dpiv[2];
-  int piv[2];
+  // T-server Gauss-Jordan: pivot q's multipliers are in srv.v[q][r]; per row r
+  // its pivot index copy, release counter, and the reciprocal of the pivot
+  // it became
+  int gpiv[kPB][kPB];
+  int gflag[kPB];
+  double2 drow[kPB];
+  int gj_fail;  // a Gauss-Jordan wait gave up
   int perm[kPB], pinv[kPB];
 };
 
@@ -742,63 +753,100 @@ __device__ void panel_role(const PersistParams& p, Shared& sh, const Sync& sy, i
 // T-server CTA
 // ---------------------------------------------------------------------------
 // Gauss-Jordan inversion of the 32x32 pivot block with partial pivoting,
-// register resident: lane r of warp w holds row r, columns [NC*w, NC*w+NC)
-// (32/NC warps).  The pivot search is one redux.sync over single-precision
-// magnitudes packed with the lane index; every candidate lane forms its
-// reciprocal while the search runs and the winner's reaches the other warps
-// through shared memory together with the pivot column (one barrier per
-// pivot).  The update is branch-free.  Row interchanges are implicit:
-//     inv[pinv[r]][perm[c]] = a(r, c),   perm[q] = row chosen at step q.
-template <int NC>
-__device__ __forceinline__ void gj_block(const PersistParams& p, Shared& sh, double2 (&a)[NC], int jn, int t,
-                                         int bar_id) {
-  constexpr int kWarps = kPB / NC;
+// register resident: lane r of warp w holds row r, columns [4w, 4w+4).  The
+// block is padded with the identity beyond its jn valid rows and columns, so
+// all 32 pivots run (a padding column is a unit vector whose pivot is its
+// own padding row; the result is the inverse padded with the identity).
+//
+// Rows are kept unscaled: after pivot q (row pv, reciprocal d of the pivot
+// value, multipliers m(r) = a(r,q) d for r != pv, m(pv) = 0) every column c
+// of every warp takes the one complex FMA  a(r,c) -= m(r) a(pv,c), the pivot
+// column becomes (-m, with 1 in row pv), and row r is multiplied by the d of
+// the pivot it became only at the end.
+//
+// Warp w chooses the pivots of its own four columns and runs ahead: for each
+// one it publishes m(r), pv (and d in lane pv) with a release store of its
+// own row's counter, lane by lane, and goes on at once; every warp applies
+// the pivots in order, each lane waiting (bounded) on its own row's counter,
+// so the chain from one pivot to the next crosses warps only at the
+// four-column block boundaries.  Pivot search: one redux.sync over
+// single-precision magnitudes packed with the lane index, the reciprocal
+// formed speculatively by every lane meanwhile.  Row interchanges are
+// implicit:  inv[pinv[r]][perm[c]] = a(r, c),  perm[q] = row chosen at q.
+// Returns false in every lane if a wait gave up (abort or timeout).
+__device__ __forceinline__ bool gj_ahead(const PersistParams& p, Shared& sh, double2 (&a)[4], int t) {
+  constexpr int NC = 4;
   const int lane = t & 31, warp = t >> 5;
   unsigned used = 0;
-  for (int q = 0; q < jn; q++) {
-    const int b = q & 1;
-    if (warp == q / NC) {
-      const int cq = q % NC;
-      double2 vq = a[0];
+  bool sing = false, ok = true;
+  for (int b = 0; b < kPB / NC; b++) {
+    if (warp == b) {
 #pragma unroll
-      for (int c = 1; c < NC; c++) vq = (c == cq) ? a[c] : vq;
-      const double2 dq = crecip_fast(vq);  // speculative: used only if this lane wins
-      const float fx = (float)vq.x, fy = (float)vq.y;
-      const float mag = fx * fx + fy * fy;
-      const bool elig = (lane < jn) && !((used >> lane) & 1u);
-      const unsigned key = elig ? ((__float_as_uint(mag) & ~63u) | (unsigned)(32 - lane)) : 0u;
-      const unsigned best = __reduce_max_sync(kFull, key);
-      const int pv = 32 - (int)(best & 63u);
-      double2 d = cmk(__shfl_sync(kFull, dq.x, pv), __shfl_sync(kFull, dq.y, pv));
-      const float magp = __uint_as_float(best & ~63u);  // the winner's |v|^2 (single precision)
-      if (!(magp >= 1e-29f && magp <= 1e29f)) {          // warp-uniform, rare: exact reciprocal
-        const double2 vp = cmk(__shfl_sync(kFull, vq.x, pv), __shfl_sync(kFull, vq.y, pv));
-        d = cinv(vp);
-      }
-      sh.fcol[b][lane] = vq;
-      if (lane == 0) {
-        sh.piv[b] = pv;
-        sh.dpiv[b] = d;
-        sh.perm[q] = pv;
-        if ((best >> 6) == 0u || !isfinite(d.x) || !isfinite(d.y)) atomicOr(p.status, kStatusSingular);
-      }
-    }
-    bar_sync(bar_id, kWarps * 32);
-    const int pv = sh.piv[b];
-    const double2 f = sh.fcol[b][lane];
-    const double2 d = sh.dpiv[b];
-    used |= 1u << pv;
-    const bool me = (lane == pv);
+      for (int cq = 0; cq < NC; cq++) {
+        const int q = b * NC + cq;
+        const double2 vq = a[cq];
+        const double2 dq = crecip_nr(vq);  // speculative: used only if this lane wins
+        const float fx = (float)vq.x, fy = (float)vq.y;
+        const float mag = fx * fx + fy * fy;
+        const bool elig = !((used >> lane) & 1u);
+        const unsigned key = elig ? ((__float_as_uint(mag) & ~63u) | (unsigned)(32 - lane)) : 0u;
+        const unsigned best = __reduce_max_sync(kFull, key);
+        const int pv = 32 - (int)(best & 63u);
+        const double2 d = cmk(__shfl_sync(kFull, dq.x, pv), __shfl_sync(kFull, dq.y, pv));
+        const bool me = lane == pv;
+        const double2 m = me ? cmk(0.0, 0.0) : cmul(vq, d);
+        sh.srv.v[q][lane] = m;
+        sh.gpiv[q][lane] = pv;
+        if (me) {
+          sh.drow[lane] = d;
+          sh.pinv[lane] = q;
+        }
+        if (lane == 0) sh.perm[q] = pv;
+        st_release_cta(&sh.gflag[lane], q + 1);
+        sing = sing || (best >> 6) == 0u || !isfinite(d.x) || !isfinite(d.y);
+        used |= 1u << pv;
 #pragma unroll
-    for (int c = 0; c < NC; c++) {
-      const bool isq = (warp * NC + c == q);
-      const double2 pr = cmk(__shfl_sync(kFull, a[c].x, pv), __shfl_sync(kFull, a[c].y, pv));
-      const double2 sp = isq ? d : cmul(pr, d);
-      const double2 base = isq ? cmk(0.0, 0.0) : a[c];
-      const double2 upd = csub(base, cmul(f, sp));
-      a[c] = me ? sp : upd;
+        for (int c = 0; c < NC; c++) {
+          if (c == cq) {
+            a[c] = me ? cmk(1.0, 0.0) : cneg(m);
+          } else {
+            const double2 pr = cmk(__shfl_sync(kFull, a[c].x, pv), __shfl_sync(kFull, a[c].y, pv));
+            a[c] = cmk(fma(-m.x, pr.x, fma(m.y, pr.y, a[c].x)), fma(-m.x, pr.y, fma(-m.y, pr.x, a[c].y)));
+          }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int cq = 0; cq < NC; cq++) {
+        const int q = b * NC + cq;
+        if (ld_acquire_cta(&sh.gflag[lane]) <= q) {
+          const long long t0 = clock64();
+          for (int spins = 1;; spins++) {
+            if (ld_acquire_cta(&sh.gflag[lane]) > q) break;
+            if ((spins & 63) == 0 && give_up(p, t0)) {
+              ok = false;
+              break;
+            }
+          }
+        }
+        const double2 m = sh.srv.v[q][lane];
+        const int pv = sh.gpiv[q][lane] & 31;
+        used |= 1u << pv;
+#pragma unroll
+        for (int c = 0; c < NC; c++) {
+          const double2 pr = cmk(__shfl_sync(kFull, a[c].x, pv), __shfl_sync(kFull, a[c].y, pv));
+          a[c] = cmk(fma(-m.x, pr.x, fma(m.y, pr.y, a[c].x)), fma(-m.x, pr.y, fma(-m.y, pr.x, a[c].y)));
+        }
+      }
     }
   }
+  // every lane has acquired its own row's counter for all 32 pivots, so the
+  // reciprocal of the pivot its row became is visible to it
+  const double2 dr = sh.drow[lane];
+#pragma unroll
+  for (int c = 0; c < NC; c++) a[c] = cmul(a[c], dr);
+  if (sing && lane == 0) atomicOr(p.status, kStatusSingular);
+  return __all_sync(kFull, ok);
 }
 
 // Cout = Cin + alpha * A B for padded 32x32 complex blocks in shared memory
@@ -902,7 +950,8 @@ __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, 
         sh.srv.a3[r][c] = c < jn ? v3[u] : cmk(0.0, 0.0);
       }
     }
-    if (t < kPB) sh.perm[t] = t;
+    if (t < kPB) sh.gflag[t] = 0;
+    if (t == 0) sh.gj_fail = 0;
     bar_sync(kBarMath, kServerThreads);
     if (t == 0) {
       if (k == 0) st_release(sy.d_used, s);
@@ -919,15 +968,13 @@ __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, 
     double2 a[4];
 #pragma unroll
     for (int c = 0; c < 4; c++) a[c] = sh.srv.a1[lane][warp * 4 + c];
-    gj_block<4>(p, sh, a, jn, t, kBarMath);
-    // perm is complete once the last pivot's barrier has passed
-    if (t < kPB) sh.pinv[sh.perm[t]] = t;
+    if (!gj_ahead(p, sh, a, t)) sh.gj_fail = 1;
     if (t == 0) {
       trace_ev(p, s, kTrSrvGJ);
       sh.panel_abort = (s >= 2) ? !wait_ge(p, sy.t_cons + par, ntiles * (s >> 1)) : 0;
     }
     bar_sync(kBarMath, kServerThreads);
-    if (sh.panel_abort) return;
+    if (sh.panel_abort || sh.gj_fail) return;
     double2* tb = p.tbuf + (size_t)par * kPB * kPB;
     const int rr = sh.pinv[lane];
 #pragma unroll
