@@ -48,7 +48,8 @@ namespace {
 
 constexpr int kPB = 32;  // pivot block width
 constexpr int kPanelWarps = 4, kPanelThreads = kPanelWarps * 32;  // one warpgroup
-constexpr int kBarMath = 1, kBarPanel = 2, kBarPub = 3, kBarDjj = 4, kBarSrv = 5;  // named barriers
+constexpr int kBarMath = 1, kBarPanel = 2, kBarPub = 3, kBarDjj = 4, kBarSrv = 5, kBarPre0 = 6,
+              kBarPre1 = 7;  // named barriers
 constexpr int kMaxTile = 96;
 constexpr int kServerThreads = 256;  // the math warpgroups of the T-server CTA
 constexpr unsigned kFull = 0xffffffffu;
@@ -209,21 +210,24 @@ __device__ bool warp_wait_all(const PersistParams& p, const int* flags, int coun
 // is kept per step parity: the same-parity value can only advance after the
 // server consumed the previous one, so "flag >= s" means "published for s".
 struct Sync {
-  int *pc_flag, *row_flag, *t_flag, *u_flag, *d_flag, *srv_flag, *d_used;
-  int *pc_cons, *row_cons, *t_cons, *u_cons, *srv_cons;
+  int *pc_flag, *pre_flag, *t_flag, *u_flag, *d_flag, *srv_flag, *d_used, *rowp_flag, *srv2_flag;
+  int *pc_cons, *pre_cons, *t_cons, *u_cons, *srv_cons, *pcp_cons;
   __device__ explicit Sync(const PersistParams& p) {
     pc_flag = p.flags;
-    row_flag = pc_flag + p.TR;
-    t_flag = row_flag + p.TC;
+    pre_flag = pc_flag + p.TR;  // [2][TC]: per parity (a slice start publishes two steps at once)
+    t_flag = pre_flag + 2 * p.TC;
     u_flag = t_flag + 1;
     d_flag = u_flag + p.TR * p.TC;
     srv_flag = d_flag + 1;
     d_used = srv_flag + 2;
+    rowp_flag = d_used + 1;  // [TC][TR]: rows of the step in panel I's share of tile column Cq
+    srv2_flag = rowp_flag + p.TR * p.TC;  // [2]: block (J_s2, J_s1), possibly from another tile column
     pc_cons = p.cons;
-    row_cons = pc_cons + 2 * p.TR;
-    t_cons = row_cons + 2 * p.TC;
+    pre_cons = pc_cons + 2 * p.TR;
+    t_cons = pre_cons + 2 * p.TC;
     u_cons = t_cons + 2;
     srv_cons = u_cons + 2 * p.TC;
+    pcp_cons = srv_cons + 2;  // [2]: panels done reading the pivot columns of a step
   }
 };
 
@@ -322,12 +326,14 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
   const int tr0 = I * BM, tc0 = Cq * BN;  // tile origin
 
   // Publication sets.  After the update of step s the warps holding pieces
-  // of step s1 = s+1 publish them: the pivot rows / columns of s1 (glob), at
-  // a slice start the first pivot block (djj), and, when s2 = s1+1 is in the
-  // same slice, three 32x32 blocks of W for the T-server (srv).  Membership
-  // depends only on the warp's row / column range, so every warp evaluates
-  // it for every warp of the CTA (barrier counts, flag-releasing lead).
-  enum { kSetGlob, kSetDjj, kSetSrv };
+  // of later steps publish them: the pivot columns of s1 = s+1 (pc), the
+  // rows J_{s1+1} (pre: the panels update them by step s1 into the pivot
+  // rows of s1+1), at a slice start also the rows J_{s1} and the first pivot
+  // block (djj), and, when s2 = s1+1 is in the same slice, the 32x32 blocks
+  // (J_s2, J_s2) and (J_s2, J_s1) of W for the T-server (srv).  Membership depends only on
+  // the warp's row / column range, so every warp evaluates it for every warp
+  // of the CTA (barrier counts, flag-releasing lead).
+  enum { kSetPc, kSetPre, kSetDjj, kSetSrv };
   auto in_set = [&](int kind, int w, int s1) {
     const int w1 = (s1 % p.NB) * kPB, w2 = w1 + kPB;
     const int rb = tr0 + (w >> 2) * Tile::WR, cb = tc0 + (w & 3) * Tile::WC;
@@ -335,7 +341,7 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
     const bool c1 = (w1 + kPB > cb) && (w1 < cb + Tile::WC);
     const bool r2 = (w2 + kPB > rb) && (w2 < rb + Tile::WR);
     const bool c2 = (w2 + kPB > cb) && (w2 < cb + Tile::WC);
-    return kind == kSetGlob ? (r1 || c1) : kind == kSetDjj ? (r1 && c1) : (r2 && c2);
+    return kind == kSetPc ? c1 : kind == kSetPre ? r1 : kind == kSetDjj ? (r1 && c1) : (r2 && (c1 || c2));
   };
   auto pub_set = [&](int kind, int s1, int* lead) {
     int n = 0;
@@ -443,40 +449,24 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
       st_release(sy.d_flag, s1);
     }
   };
-  // the pivot rows (rowbuf) and columns (pcbuf) of step s1; the lead warp
-  // releases the flags after every publishing warp wrote
-  auto publish_glob = [&](int s1) {
+  // the pivot columns (pcbuf) of step s1; the lead warp releases the flag
+  // after every publishing warp wrote
+  auto publish_pc = [&](int s1) {
     const int w0 = (s1 % p.NB) * kPB;
     const int jnn = min(kPB, p.N - w0);
     const int par = s1 & 1;
     int lead;
-    const int n = pub_set(kSetGlob, s1, &lead);
+    const int n = pub_set(kSetPc, s1, &lead);
     if (warp == lead && t.lane == 0) trace_ev(p, s1 - 1, kTrGlobEnter);
-    const bool any_r = t.r_base + Tile::WR > w0 && t.r_base < w0 + kPB;
-    const bool any_c = t.c_base + Tile::WC > w0 && t.c_base < w0 + kPB;
     int ok = 1;
-    if (t.lane == 0 && s1 >= 2) {
-      if (any_r) ok &= wait_ge(p, sy.row_cons + par * p.TC + Cq, p.TR * (s1 >> 1));
-      if (any_c && ok) ok &= wait_ge(p, sy.pc_cons + par * p.TR + I, p.TC * (s1 >> 1));
+    if (t.lane == 0 && s1 >= 2) {  // the math warps and every panel are done with step s1-2's
+      ok = wait_ge(p, sy.pc_cons + par * p.TR + I, p.TC * (s1 >> 1));
+      ok = ok && wait_ge(p, sy.pcp_cons + par, p.TR * p.TC * (s1 >> 1));
     }
     ok = __shfl_sync(kFull, ok, 0);
     if (ok) {
-      // pivot rows: rowbuf[k][c - tc0], zero beyond the last pivot row
-      double2* rowb = p.rowbuf + ((size_t)par * p.TC + Cq) * (kPB * BN) + (t.c_base - tc0 + lc);
-#pragma unroll
-      for (int mi = 0; mi < MI; mi++) {
-        if (!row_in(mi, w0)) continue;
-        const int kr = t.r_base + mi * 8 + lr - w0;
-        const bool valid = kr < jnn;
-        double2* q = rowb + kr * BN;
-#pragma unroll
-        for (int ni = 0; ni < NI; ni++)
-#pragma unroll
-          for (int h = 0; h < 2; h++)
-            __stcg(q + ni * 8 + h, valid ? cmk(t.acc[mi][ni][h], t.acc[mi][ni][2 + h]) : cmk(0.0, 0.0));
-      }
-      // pivot columns: Pc = [-W(i, J) ; +I on the pivot rows], zero beyond the
-      // last pivot column and below row R, stored in the swizzled [BM][32] layout
+      // Pc = [-W(i, J) ; +I on the pivot rows], zero beyond the last pivot
+      // column and below row R, stored in the swizzled [BM][32] layout
       double2* pcb = p.pcbuf + ((size_t)par * p.TR + I) * (BM * kPB) + (t.r_base - tr0 + lr) * kPB;
 #pragma unroll
       for (int ni = 0; ni < NI; ni++) {
@@ -500,13 +490,43 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
     if (warp == lead && t.lane == 0) trace_ev(p, s1 - 1, kTrGlobStored);
     const int all_ok = !bar_or(kBarPub, n * 32, !ok);
     if (warp == lead && t.lane == 0 && all_ok) {  // an aborted publish never releases anything
-      if (w0 >= tr0 && w0 < tr0 + BM) st_release(sy.row_flag + Cq, s1);
-      if (w0 >= tc0 && w0 < tc0 + BN) st_release(sy.pc_flag + I, s1);
+      st_release(sy.pc_flag + I, s1);
       trace_ev(p, s1 - 1, kTrMathPublished);
     }
   };
-  // block (J_s2, J_s2) of the current W, s2 = s1+1, for the T-server's Schur
-  // update of step s2 (padded with the identity beyond the last pivot row)
+  // rows J_x of the current W (prebuf[x & 1][Cq][k][c - tc0], zero beyond the
+  // last pivot row) for the panels of tile column Cq
+  auto publish_pre = [&](int x, int bar_id) {
+    const int w0 = (x % p.NB) * kPB;
+    const int jnn = min(kPB, p.N - w0);
+    const int par = x & 1;
+    int lead;
+    const int n = pub_set(kSetPre, x, &lead);
+    int ok = 1;
+    if (t.lane == 0 && x >= 2) ok = wait_ge(p, sy.pre_cons + par * p.TC + Cq, p.TR * (x >> 1));
+    ok = __shfl_sync(kFull, ok, 0);
+    if (ok) {
+      double2* rowb = p.prebuf + ((size_t)par * p.TC + Cq) * (kPB * BN) + (t.c_base - tc0 + lc);
+#pragma unroll
+      for (int mi = 0; mi < MI; mi++) {
+        if (!row_in(mi, w0)) continue;
+        const int kr = t.r_base + mi * 8 + lr - w0;
+        const bool valid = kr < jnn;
+        double2* q = rowb + kr * BN;
+#pragma unroll
+        for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+          for (int h = 0; h < 2; h++)
+            __stcg(q + ni * 8 + h, valid ? cmk(t.acc[mi][ni][h], t.acc[mi][ni][2 + h]) : cmk(0.0, 0.0));
+      }
+    }
+    const int all_ok = !bar_or(bar_id, n * 32, !ok);
+    if (warp == lead && t.lane == 0 && all_ok) st_release(sy.pre_flag + par * p.TC + Cq, x);
+  };
+  // blocks (J_s2, J_s2) (padded with the identity beyond the last pivot row)
+  // and (J_s2, J_s1) (zero rows there) of the current W, s2 = s1+1, for the
+  // T-server's Schur update of step s2; published first after the update,
+  // the server's chain waits for them
   auto publish_srv = [&](int s1) {
     const int s2 = s1 + 1;
     const int w1 = (s1 % p.NB) * kPB, w2 = w1 + kPB;
@@ -519,22 +539,27 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
     if (t.lane == 0 && s2 >= 2) ok = wait_ge(p, sy.srv_cons + par, s2 >> 1);
     ok = __shfl_sync(kFull, ok, 0);
     if (ok) {
-      store_block(p.srvbuf + (size_t)par * kPB * kPB, w2, w2, jn2, jn2, true);
+      store_block(p.srvbuf + (size_t)par * 2 * kPB * kPB, w2, w2, jn2, jn2, true);
+      store_block(p.srvbuf + ((size_t)par * 2 + 1) * kPB * kPB, w2, w1, jn2, kPB, false);
     }
     if (warp == lead && t.lane == 0) trace_ev(p, s1 - 1, kTrSrvPubStored);
     const int all_ok = !bar_or(kBarSrv, n * 32, !ok);
     if (warp == lead && t.lane == 0 && all_ok) {
-      st_release(sy.srv_flag + par, s2);
+      if (w2 >= tc0 && w2 < tc0 + BN) st_release(sy.srv_flag + par, s2);
+      if (w1 >= tc0 && w1 < tc0 + BN) st_release(sy.srv2_flag + par, s2);
       trace_ev(p, s1 - 1, kTrSrvPubDone);
     }
   };
-  // every piece of step s1 this warp holds; at a slice start (kernel start or
-  // after the slice assembly) also the first pivot block
+  // every piece of later steps this warp holds after the update of step
+  // s1 - 1; at a slice start (kernel start or after the slice assembly) also
+  // the rows J_{s1} and the first pivot block
   auto publish = [&](int s1, bool slice_start) {
-    const bool with_srv = (s1 % p.NB) + 1 <= p.NB - 1;  // step s1 + 1 is in the same slice
+    const bool next_in_slice = (s1 % p.NB) + 1 < p.NB;  // step s1 + 1 is in the same slice
     if (slice_start && in_set(kSetDjj, warp, s1)) publish_djj(s1);
-    if (in_set(kSetGlob, warp, s1)) publish_glob(s1);
-    if (with_srv && in_set(kSetSrv, warp, s1)) publish_srv(s1);
+    if (next_in_slice && in_set(kSetSrv, warp, s1)) publish_srv(s1);
+    if (in_set(kSetPc, warp, s1)) publish_pc(s1);
+    if (slice_start && in_set(kSetPre, warp, s1)) publish_pre(s1, kBarPre0);
+    if (next_in_slice && in_set(kSetPre, warp, s1 + 1)) publish_pre(s1 + 1, kBarPre1);
   };
 
   load_tile();
@@ -659,93 +684,195 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
 }
 
 // ---------------------------------------------------------------------------
-// tile CTA, panel warpgroup: U_s(:, my columns) = T_s * W(J_s, my columns)
+// tile CTA, panel warpgroup: U_s(:, my columns) = T_s * W(J_s, my columns),
+// then the pivot rows of step s+1 in my columns one step ahead
 // ---------------------------------------------------------------------------
+// The pivot rows of step s+1 after the update of step s are
+//     W^(s)(J_{s+1}, c) = P_{s+1}(c) [c not in J_s] + Pc_s(J_{s+1}, :) U_s(:, c)
+// with P_{s+1} = W^(s-1)(J_{s+1}, :), published by the math warps holding
+// those rows after step s-1, and Pc_s = -W^(s-1)(:, J_s) the pivot columns
+// of step s: the same update the math warps apply to their registers (whose
+// rows J_{s+1} are then never read again).  Computing them here, right after
+// U_s, takes the math pass of step s off the path from T_s to U_{s+1}.
+// The share of panel I is columns [cs, cs + w) of tile column Cq.
 template <int BM, int BN>
 __device__ void panel_role(const PersistParams& p, Shared& sh, const Sync& sy, int I, int Cq) {
   const int t = threadIdx.x - Cfg<BM, BN>::MathThreads;
   const int lane = t & 31, warp = t >> 5;
   const int S = p.L * p.NB;
-  const int per = (BN + p.TR - 1) / p.TR;  // my columns of U(Cq): [cs, cs + w)
+  const int per = (BN + p.TR - 1) / p.TR;
   const int cs = I * per;
   const int w = max(0, min(per, BN - cs));
-  for (int s = 0; s < S; s++) {
-    const int k = s % p.NB;
-    const int j0 = k * kPB, jn = min(kPB, p.N - j0);
-    const int par = s & 1;
+  constexpr int kPer = kPB * kPB / kPanelThreads;
+  const int r = warp * 8 + (lane >> 2);  // warp w computes rows [8w, 8w+8), one 8-column tile at a time
+
+  // rows of step s1 = s+1 in my columns -> rowbuf[s1 & 1]: P_{s1} updated by
+  // step s, or P_{s1} itself when s1 starts a slice (s = -1: the first step)
+  auto lookahead = [&](int s) -> bool {
+    const int s1 = s + 1;
+    const bool upd = s >= 0 && (s % p.NB) + 1 < p.NB;
+    const int par = s & 1, par1 = s1 & 1;
+    const int w1 = (s1 % p.NB) * kPB, jn1 = min(kPB, p.N - w1);
+    const int I1 = w1 / BM;
+    const int j0 = upd ? (s % p.NB) * kPB : 0, jn = upd ? min(kPB, p.N - j0) : 0;
     if (t == 0) {
-      trace_ev(p, s, kTrPanelStart);
-      int ok = wait_ge(p, sy.t_flag, s);
-      ok = ok && wait_ge(p, sy.row_flag + Cq, s);
+      int ok = wait_ge(p, sy.pre_flag + par1 * p.TC + Cq, s1);
+      if (ok && upd) ok = wait_ge(p, sy.pc_flag + I1, s);
       sh.panel_abort = !ok;
-      trace_ev(p, s, kTrPanelUin);
     }
     bar_sync(kBarPanel, kPanelThreads);
-    if (sh.panel_abort) return;
-    const double2* tb = p.tbuf + (size_t)par * kPB * kPB;
-    const double2* rows = p.rowbuf + ((size_t)par * p.TC + Cq) * (kPB * BN);
-    double2* ub = p.ubuf + ((size_t)par * p.TC + Cq) * (kPB * BN);
-    constexpr int kPer = kPB * kPB / kPanelThreads;
-    bool waited_u = false;
-    for (int cc = 0; cc < w; cc += kPB) {
-      const int wc = min(kPB, w - cc);
-      // the loads of T (first chunk) and of this chunk of pivot rows, each
-      // batch in flight at once
-      double2 v[kPer];
-      if (cc == 0) {
-#pragma unroll
-        for (int u = 0; u < kPer; u++) v[u] = __ldcg(tb + t + u * kPanelThreads);
-#pragma unroll
-        for (int u = 0; u < kPer; u++) sh.T[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
-      }
+    if (sh.panel_abort) return false;
+    double2 v[kPer];
+    if (upd && w > 0) {  // Pc_s(J_{s1}, :) -> sh.T (T_s is not needed any more)
+      const double2* pcb = p.pcbuf + ((size_t)par * p.TR + I1) * (BM * kPB) + (size_t)(w1 - I1 * BM) * kPB;
 #pragma unroll
       for (int u = 0; u < kPer; u++) {
         const int e = t + u * kPanelThreads, q = e / kPB, c = e % kPB;
-        v[u] = (c < wc) ? __ldcg(rows + q * BN + cs + cc + c) : cmk(0.0, 0.0);
+        v[u] = __ldcg(pcb + q * kPB + (c ^ ((q & 1) << 2)));
       }
 #pragma unroll
-      for (int u = 0; u < kPer; u++) sh.Mr[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
+      for (int u = 0; u < kPer; u++) sh.T[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
+    }
+    const double2* pre = p.prebuf + ((size_t)par1 * p.TC + Cq) * (kPB * BN);
+    const double2* ub = p.ubuf + ((size_t)(par & 1) * p.TC + Cq) * (kPB * BN);
+    double2* rowo = p.rowbuf + ((size_t)par1 * p.TC + Cq) * (kPB * BN);
+    for (int cc = 0; cc < w; cc += kPB) {
+      const int wc = min(kPB, w - cc);
+      if (upd) {  // U_s(:, this chunk), as stored for the math warps, -> sh.Mr
+#pragma unroll
+        for (int u = 0; u < kPer; u++) {
+          const int e = t + u * kPanelThreads, q = e / kPB, c = e % kPB;
+          v[u] = (c < wc) ? __ldcg(ub + swzB<BN>(q, cs + cc + c)) : cmk(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < kPer; u++) sh.Mr[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
+      }
       bar_sync(kBarPanel, kPanelThreads);
-      if (!waited_u) {
-        if (t == 0) sh.panel_abort = (s >= 2) ? !wait_ge(p, sy.u_cons + par * p.TC + Cq, p.TR * (s >> 1)) : 0;
-        bar_sync(kBarPanel, kPanelThreads);
-        if (sh.panel_abort) return;
-        waited_u = true;
-      }
-      // warp w owns rows [8w, 8w+8), one m8n8k4 column tile of 8 at a time
-      // (T_s is padded with the identity and the pivot rows with zeros beyond jn)
-      const int r = warp * 8 + (lane >> 2);
       for (int nt = 0; nt * 8 < wc; nt++) {
-        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        double acc[4];
 #pragma unroll
-        for (int kk = 0; kk < kPB / 4; kk++) {
-          const double2 a = sh.T[r][kk * 4 + (lane & 3)];
-          const double2 bb = sh.Mr[kk * 4 + (lane & 3)][nt * 8 + (lane >> 2)];
-          dmma(acc[0], acc[1], a.x, bb.x);
-          dmma(acc[2], acc[3], a.x, bb.y);
-          dmma(acc[0], acc[1], -a.y, bb.y);
-          dmma(acc[2], acc[3], a.y, bb.x);
+        for (int h = 0; h < 2; h++) {
+          const int c = nt * 8 + (lane & 3) * 2 + h;
+          const int64_t gc = (int64_t)Cq * BN + cs + cc + c;
+          double2 pv = (c < wc) ? __ldcg(pre + r * BN + cs + cc + c) : cmk(0.0, 0.0);
+          if (gc >= j0 && gc < j0 + jn) pv = cmk(0.0, 0.0);  // columns J_s read as zero
+          acc[h] = pv.x;
+          acc[2 + h] = pv.y;
+        }
+        if (upd) {
+#pragma unroll
+          for (int kk = 0; kk < kPB / 4; kk++) {
+            const double2 a = sh.T[r][kk * 4 + (lane & 3)];
+            const double2 bb = sh.Mr[kk * 4 + (lane & 3)][nt * 8 + (lane >> 2)];
+            dmma(acc[0], acc[1], a.x, bb.x);
+            dmma(acc[2], acc[3], a.x, bb.y);
+            dmma(acc[0], acc[1], -a.y, bb.y);
+            dmma(acc[2], acc[3], a.y, bb.x);
+          }
         }
 #pragma unroll
         for (int h = 0; h < 2; h++) {
           const int c = nt * 8 + (lane & 3) * 2 + h;
           if (c >= wc) continue;
           const int64_t gc = (int64_t)Cq * BN + cs + cc + c;
-          double2 v = cmk(acc[h], acc[2 + h]);
-          if (r >= jn || gc >= p.C) v = cmk(0.0, 0.0);
-          else if (gc >= j0 && gc < j0 + jn) v = sh.T[r][gc - j0];
-          __stcg(ub + swzB<BN>(r, cs + cc + c), v);
+          const double2 o = (r >= jn1 || gc >= p.C) ? cmk(0.0, 0.0) : cmk(acc[h], acc[2 + h]);
+          __stcg(rowo + r * BN + cs + cc + c, o);
         }
       }
       bar_sync(kBarPanel, kPanelThreads);
     }
-    bar_sync(kBarPanel, kPanelThreads);  // every read of T and of the pivot rows is done
     if (t == 0) {
-      atomicAdd(sy.t_cons + par, 1);
-      atomicAdd(sy.row_cons + par * p.TC + Cq, 1);
-      st_release(sy.u_flag + Cq * p.TR + I, s);
-      trace_ev(p, s, kTrPanelUout);
+      atomicAdd(sy.pre_cons + par1 * p.TC + Cq, 1);
+      if (s >= 0) atomicAdd(sy.pcp_cons + par, 1);
+      st_release(sy.rowp_flag + Cq * p.TR + I, s1);
     }
+    return true;
+  };
+
+  for (int s = -1; s < S; s++) {  // s = -1: only the pivot rows of the first step
+    if (s >= 0) {
+      const int k = s % p.NB;
+      const int j0 = k * kPB, jn = min(kPB, p.N - j0);
+      const int par = s & 1;
+      const double2* tb = p.tbuf + (size_t)par * kPB * kPB;
+      const double2* rows = p.rowbuf + ((size_t)par * p.TC + Cq) * (kPB * BN);
+      double2* ub = p.ubuf + ((size_t)par * p.TC + Cq) * (kPB * BN);
+      // chunk 0 of my pivot rows (written by this warpgroup one step earlier)
+      // goes to shared memory before T_s is awaited
+      double2 v[kPer];
+      if (w > 0) {
+#pragma unroll
+        for (int u = 0; u < kPer; u++) {
+          const int e = t + u * kPanelThreads, q = e / kPB, c = e % kPB;
+          v[u] = (c < min(kPB, w)) ? __ldcg(rows + q * BN + cs + c) : cmk(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < kPer; u++) sh.Mr[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
+      }
+      if (t == 0) {
+        trace_ev(p, s, kTrPanelStart);
+        sh.panel_abort = !wait_ge(p, sy.t_flag, s);
+        trace_ev(p, s, kTrPanelUin);
+      }
+      bar_sync(kBarPanel, kPanelThreads);
+      if (sh.panel_abort) return;
+      bool waited_u = false;
+      for (int cc = 0; cc < w; cc += kPB) {
+        const int wc = min(kPB, w - cc);
+        if (cc == 0) {
+#pragma unroll
+          for (int u = 0; u < kPer; u++) v[u] = __ldcg(tb + t + u * kPanelThreads);
+#pragma unroll
+          for (int u = 0; u < kPer; u++) sh.T[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
+        } else {
+#pragma unroll
+          for (int u = 0; u < kPer; u++) {
+            const int e = t + u * kPanelThreads, q = e / kPB, c = e % kPB;
+            v[u] = (c < wc) ? __ldcg(rows + q * BN + cs + cc + c) : cmk(0.0, 0.0);
+          }
+#pragma unroll
+          for (int u = 0; u < kPer; u++) sh.Mr[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
+        }
+        bar_sync(kBarPanel, kPanelThreads);
+        if (!waited_u) {
+          if (t == 0) sh.panel_abort = (s >= 2) ? !wait_ge(p, sy.u_cons + par * p.TC + Cq, p.TR * (s >> 1)) : 0;
+          bar_sync(kBarPanel, kPanelThreads);
+          if (sh.panel_abort) return;
+          waited_u = true;
+        }
+        // T_s is padded with the identity and the pivot rows with zeros beyond jn
+        for (int nt = 0; nt * 8 < wc; nt++) {
+          double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+          for (int kk = 0; kk < kPB / 4; kk++) {
+            const double2 a = sh.T[r][kk * 4 + (lane & 3)];
+            const double2 bb = sh.Mr[kk * 4 + (lane & 3)][nt * 8 + (lane >> 2)];
+            dmma(acc[0], acc[1], a.x, bb.x);
+            dmma(acc[2], acc[3], a.x, bb.y);
+            dmma(acc[0], acc[1], -a.y, bb.y);
+            dmma(acc[2], acc[3], a.y, bb.x);
+          }
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            const int c = nt * 8 + (lane & 3) * 2 + h;
+            if (c >= wc) continue;
+            const int64_t gc = (int64_t)Cq * BN + cs + cc + c;
+            double2 o = cmk(acc[h], acc[2 + h]);
+            if (r >= jn || gc >= p.C) o = cmk(0.0, 0.0);
+            else if (gc >= j0 && gc < j0 + jn) o = sh.T[r][gc - j0];
+            __stcg(ub + swzB<BN>(r, cs + cc + c), o);
+          }
+        }
+        bar_sync(kBarPanel, kPanelThreads);
+      }
+      bar_sync(kBarPanel, kPanelThreads);  // every read of T is done
+      if (t == 0) {
+        atomicAdd(sy.t_cons + par, 1);
+        st_release(sy.u_flag + Cq * p.TR + I, s);
+        trace_ev(p, s, kTrPanelUout);
+      }
+    }
+    if (s + 1 < S && !lookahead(s)) return;
   }
 }
 
@@ -891,63 +1018,73 @@ __device__ __forceinline__ void blk_gemm(const Blk& A, const Blk& B, const Blk* 
 
 // the 8 math warps of the server CTA form and invert every pivot block one
 // step ahead of the bulk update.  For step s (not the first of its slice):
-//   a1 = W^{(s-2)}(J_s, J_s)      from srvbuf (published after step s-2)
-//   a2 = W^{(s-2)}(J_s, J_{s-1})  = -(pivot columns of step s-1, rows J_s)
-//   a3 = W^{(s-2)}(J_{s-1}, J_s)  =   pivot rows of step s-1, columns J_s
-// The pivot buffers of step s-1 stay valid until they are published for
-// step s+1, which needs T_s from this CTA.
+//   a3 = W^{(s-2)}(J_{s-1}, J_s)  = pivot rows of step s-1 (panels), columns J_s
+//   a1 = W^{(s-2)}(J_s, J_s)      } from srvbuf, published first by the math
+//   a2 = W^{(s-2)}(J_s, J_{s-1})  } warps after the update of step s-2
+// and W^{(s-1)}(J_s, J_s) = a1 - a2 (T_{s-1} a3); the product V = T_{s-1} a3
+// is formed while a1 and a2 are awaited.  The pivot rows of step s-1 stay
+// valid until the panels write those of step s+1, which needs T_s.
 template <int BM, int BN>
 __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, int t) {
   const int lane = t & 31, warp = t >> 5;
   const int S = p.L * p.NB;
   const int ntiles = p.TR * p.TC;
+  constexpr int kPer = kPB * kPB / kServerThreads;
   for (int s = 0; s < S; s++) {
     const int k = s % p.NB;
     const int jn = min(kPB, p.N - k * kPB);
     const int par = s & 1;
-    if (t == 0) {
-      trace_ev(p, s, kTrPanelStart);
-      bool ok;
-      if (k == 0) {
-        ok = wait_ge(p, sy.d_flag, s);
-      } else {
-        const int w = k * kPB;
-        ok = wait_ge(p, sy.srv_flag + par, s) && wait_ge(p, sy.pc_flag + w / BM, s - 1) &&
-             wait_ge(p, sy.row_flag + w / BN, s - 1);
+    if (t == 0) trace_ev(p, s, kTrPanelStart);
+    if (k != 0) {
+      const int w = k * kPB, C2 = w / BN;
+      if (warp == 0) {  // a3 comes in shares from the TR panels of its tile column
+        const bool ok = warp_wait_all(p, sy.rowp_flag + C2 * p.TR, p.TR, nullptr, s - 1);
+        if (lane == 0) sh.panel_abort = !ok;
       }
-      sh.panel_abort = !ok;
+      bar_sync(kBarMath, kServerThreads);
+      if (sh.panel_abort) return;
+      const double2* rwb = p.rowbuf + ((size_t)(par ^ 1) * p.TC + C2) * (kPB * BN) + (w - C2 * BN);
+      double2 v3[kPer];
+#pragma unroll
+      for (int u = 0; u < kPer; u++) {
+        const int e = t + u * kServerThreads;
+        v3[u] = __ldcg(rwb + (e / kPB) * BN + e % kPB);
+      }
+#pragma unroll
+      for (int u = 0; u < kPer; u++) {
+        const int e = t + u * kServerThreads, r = e / kPB, c = e % kPB;
+        sh.srv.a3[r][c] = c < jn ? v3[u] : cmk(0.0, 0.0);
+      }
+      bar_sync(kBarMath, kServerThreads);
+      blk_gemm(sh.srv.tprev, sh.srv.a3, nullptr, 1.0, sh.srv.v, t);
+    }
+    if (t == 0) {
+      sh.panel_abort = k == 0 ? !wait_ge(p, sy.d_flag, s)
+                              : !(wait_ge(p, sy.srv_flag + par, s) && wait_ge(p, sy.srv2_flag + par, s));
       trace_ev(p, s, kTrPanelTin);
     }
     bar_sync(kBarMath, kServerThreads);
     if (sh.panel_abort) return;
     if (k == 0) {
-      constexpr int kPer = kPB * kPB / kServerThreads;
       double2 v1[kPer];
 #pragma unroll
       for (int u = 0; u < kPer; u++) v1[u] = __ldcg(p.djjbuf + t + u * kServerThreads);
 #pragma unroll
       for (int u = 0; u < kPer; u++) sh.srv.a1[(t + u * kServerThreads) / kPB][(t + u * kServerThreads) % kPB] = v1[u];
     } else {
-      const double2* sb = p.srvbuf + (size_t)par * kPB * kPB;
-      const int w = k * kPB, parq = par ^ 1;
-      const int I2 = w / BM, C2 = w / BN;
-      const double2* pcb = p.pcbuf + ((size_t)parq * p.TR + I2) * (BM * kPB) + (size_t)(w - I2 * BM) * kPB;
-      const double2* rwb = p.rowbuf + ((size_t)parq * p.TC + C2) * (kPB * BN) + (w - C2 * BN);
-      constexpr int kPer = kPB * kPB / kServerThreads;
-      double2 v1[kPer], v2[kPer], v3[kPer];
+      const double2* sb = p.srvbuf + (size_t)par * 2 * kPB * kPB;
+      double2 v1[kPer], v2[kPer];
 #pragma unroll
       for (int u = 0; u < kPer; u++) {  // all loads in flight before the first use
-        const int e = t + u * kServerThreads, r = e / kPB, c = e % kPB;
+        const int e = t + u * kServerThreads;
         v1[u] = __ldcg(sb + e);
-        v2[u] = __ldcg(pcb + r * kPB + (c ^ ((r & 1) << 2)));
-        v3[u] = __ldcg(rwb + r * BN + c);
+        v2[u] = __ldcg(sb + kPB * kPB + e);
       }
 #pragma unroll
       for (int u = 0; u < kPer; u++) {
         const int e = t + u * kServerThreads, r = e / kPB, c = e % kPB;
         sh.srv.a1[r][c] = v1[u];
-        sh.srv.a2[r][c] = r < jn ? cneg(v2[u]) : cmk(0.0, 0.0);
-        sh.srv.a3[r][c] = c < jn ? v3[u] : cmk(0.0, 0.0);
+        sh.srv.a2[r][c] = v2[u];
       }
     }
     if (t < kPB) sh.gflag[t] = 0;
@@ -958,9 +1095,7 @@ __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, 
       atomicAdd(sy.srv_cons + par, 1);
       trace_ev(p, s, kTrSrvLoaded);
     }
-    if (k != 0) {  // W^{(s-1)}(J_s,J_s) = a1 - a2 T_{s-1} a3
-      blk_gemm(sh.srv.tprev, sh.srv.a3, nullptr, 1.0, sh.srv.v, t);
-      bar_sync(kBarMath, kServerThreads);
+    if (k != 0) {  // W^{(s-1)}(J_s,J_s) = a1 - a2 V
       blk_gemm(sh.srv.a2, sh.srv.v, &sh.srv.a1, -1.0, sh.srv.a1, t);
       bar_sync(kBarMath, kServerThreads);
     }

@@ -18,13 +18,14 @@ struct PersistParams {
   const double2* st_val;
   int pc1;               // probe columns pc1, pc1 + 1 (pc1 even), -1 = none
   double2* pcbuf;        // [2][TR][BM][32]
-  double2* rowbuf;       // [2][TC][32][BN]
+  double2* rowbuf;       // [2][TC][32][BN] pivot rows of a step (written by the panels)
+  double2* prebuf;       // [2][TC][32][BN] the same rows one step earlier (written by the math warps)
   double2* tbuf;         // [2][32][32]
   double2* ubuf;         // [2][TC][32][BN]
   double2* djjbuf;       // [32][32] first pivot block of a slice, for the T-server CTA
-  double2* srvbuf;       // [2][32][32] block the T-server updates into the next pivot block
-  int* flags;            // pc[TR], row[TC], t[1], u[TC*TR], d[1], srv[2], d_used[1]  (init -1)
-  int* cons;             // pc[2][TR], row[2][TC], t[2], u[2][TC], srv[2]             (init 0)
+  double2* srvbuf;       // [2][2][32][32] blocks the T-server updates into the next pivot block
+  int* flags;  // pc[TR], pre[2][TC], t[1], u[TC*TR], d[1], srv[2], d_used[1], rowp[TC*TR], srv2[2] (init -1)
+  int* cons;   // pc[2][TR], pre[2][TC], t[2], u[2][TC], srv[2], pcp[2]                              (init 0)
   // optional snapshots of W after slice n (launch-relative) for every n with
   // n % snap_mod == snap_mod - 1, at snap + (n / snap_mod) * snap_ld, laid
   // out as M (probe columns excepted)
@@ -53,8 +54,8 @@ enum { kTrMathStart = 0, kTrMathOperands, kTrMathCopied, kTrMathPublished, kTrMa
        // T-server: end of the factorization of each 4-pivot group
        kTrSrvGroup0, kTraceEvents = kTrSrvGroup0 + 8 };
 
-inline int persist_flag_words(int TR, int TC) { return TR + TC + 1 + TR * TC + 1 + 2 + 1; }
-inline int persist_cons_words(int TR, int TC) { return 2 * TR + 2 * TC + 2 + 2 * TC + 2; }
+inline int persist_flag_words(int TR, int TC) { return TR + 2 * TC + 1 + TR * TC + 1 + 2 + 1 + TR * TC + 2; }
+inline int persist_cons_words(int TR, int TC) { return 2 * TR + 2 * TC + 2 + 2 * TC + 2 + 2; }
 
 size_t persist_smem_bytes();
 int persist_threads(int BM, int BN);

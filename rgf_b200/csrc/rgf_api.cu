@@ -594,8 +594,8 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
       const int TR = (int)((Rp + BMp - 1) / BMp), TC = (int)((Cp + BNp - 1) / BNp);
       const int nflags = persist_flag_words(TR, TC), ncons = persist_cons_words(TR, TC);
       if ((st = ensure(h->xpc, sizeof(double2) * 2 * TR * BMp * 32))) return st;
-      if ((st = ensure(h->xrow, sizeof(double2) * 2 * TC * 32 * BNp))) return st;
-      if ((st = ensure(h->xt, sizeof(double2) * 5 * 32 * 32))) return st;  // tbuf[2], djjbuf, srvbuf[2]
+      if ((st = ensure(h->xrow, sizeof(double2) * 4 * TC * 32 * BNp))) return st;  // rowbuf, prebuf
+      if ((st = ensure(h->xt, sizeof(double2) * 7 * 32 * 32))) return st;  // tbuf[2], djjbuf, srvbuf[2][2]
       if ((st = ensure(h->xu, sizeof(double2) * 2 * TC * 32 * BNp))) return st;
       if ((st = ensure(h->xsync, sizeof(int) * (nflags + ncons + 4)))) return st;
       int* flags = as<int>(h->xsync);
@@ -622,6 +622,7 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
       pp.pc1 = (int)pc1;
       pp.pcbuf = as<double2>(h->xpc);
       pp.rowbuf = as<double2>(h->xrow);
+      pp.prebuf = as<double2>(h->xrow) + (size_t)2 * TC * 32 * BNp;
       pp.tbuf = as<double2>(h->xt);
       pp.djjbuf = as<double2>(h->xt) + 2 * 32 * 32;
       pp.srvbuf = as<double2>(h->xt) + 3 * 32 * 32;
