@@ -49,7 +49,7 @@ namespace {
 constexpr int kPB = 32;  // pivot block width
 constexpr int kPanelWarps = 4, kPanelThreads = kPanelWarps * 32;  // one warpgroup
 constexpr int kBarMath = 1, kBarPanel = 2, kBarPub = 3, kBarDjj = 4, kBarSrv = 5, kBarPre0 = 6,
-              kBarPre1 = 7;  // named barriers
+              kBarPre1 = 7, kBarSrv2 = 8;  // named barriers
 constexpr int kMaxTile = 96;
 constexpr int kServerThreads = 256;  // the math warpgroups of the T-server CTA
 constexpr unsigned kFull = 0xffffffffu;
@@ -142,8 +142,11 @@ struct Shared {
       alignas(128) double2 A[kMaxTile * kPB];
       alignas(128) double2 B[kPB * kMaxTile];
     } op;
-    struct {  // T-server CTA: the three published blocks, T_{s-1}, scratch
-      Blk a1, a2, a3, tprev, v;
+    struct {  // T-server CTA: next pivot block, a3, T_{s-1}, scratch, and per
+              // step parity the blocks (J_s, J_s), (J_s, J_{s-1}) formed by
+              // the prep warps
+      Blk a1, a3, tprev, v;
+      Blk y[2][2];
     } srv;
   };
   alignas(8) unsigned long long mbar;
@@ -158,6 +161,9 @@ struct Shared {
   int gflag[kPB];
   double2 drow[kPB];
   int gj_fail;  // a Gauss-Jordan wait gave up
+  int ysig[2];  // T-server: step whose y[parity] blocks are ready (prep -> server)
+  int ycons;    // T-server: last step whose y blocks the server has read
+  int prep_abort;  // T-server CTA, prep warps: a wait gave up
   int perm[kPB], pinv[kPB];
 };
 
@@ -183,6 +189,17 @@ __device__ bool wait_ge(const PersistParams& p, const int* flag, int target) {
   for (int spins = 1;; spins++) {
     if (spins > 64) __nanosleep(32);
     if (ld_acquire(flag) >= target) return true;
+    if ((spins & 63) == 0 && give_up(p, t0)) return false;
+  }
+}
+
+// the same on a shared-memory flag (other warps of this CTA)
+__device__ bool wait_cta_ge(const PersistParams& p, const int* flag, int target) {
+  if (ld_acquire_cta(flag) >= target) return true;
+  const long long t0 = clock64();
+  for (int spins = 1;; spins++) {
+    if (spins > 64) __nanosleep(32);
+    if (ld_acquire_cta(flag) >= target) return true;
     if ((spins & 63) == 0 && give_up(p, t0)) return false;
   }
 }
@@ -461,7 +478,7 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
     int ok = 1;
     if (t.lane == 0 && s1 >= 2) {  // the math warps and every panel are done with step s1-2's
       ok = wait_ge(p, sy.pc_cons + par * p.TR + I, p.TC * (s1 >> 1));
-      ok = ok && wait_ge(p, sy.pcp_cons + par, p.TR * p.TC * (s1 >> 1));
+      ok = ok && wait_ge(p, sy.pcp_cons + par, (p.TR * p.TC + 1) * (s1 >> 1));
     }
     ok = __shfl_sync(kFull, ok, 0);
     if (ok) {
@@ -525,9 +542,9 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
   };
   // blocks (J_s2, J_s2) (padded with the identity beyond the last pivot row)
   // and (J_s2, J_s1) (zero rows there) of the current W, s2 = s1+1, for the
-  // T-server's Schur update of step s2; published first after the update,
-  // the server's chain waits for them
-  auto publish_srv = [&](int s1) {
+  // T-server's prep warps, which update them by step s2-2 (unless s2 is the
+  // second step of its slice) into the blocks of the Schur update of step s2
+  auto publish_srv = [&](int s1, int bar_id) {
     const int s2 = s1 + 1;
     const int w1 = (s1 % p.NB) * kPB, w2 = w1 + kPB;
     const int jn2 = min(kPB, p.N - w2);
@@ -543,7 +560,7 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
       store_block(p.srvbuf + ((size_t)par * 2 + 1) * kPB * kPB, w2, w1, jn2, kPB, false);
     }
     if (warp == lead && t.lane == 0) trace_ev(p, s1 - 1, kTrSrvPubStored);
-    const int all_ok = !bar_or(kBarSrv, n * 32, !ok);
+    const int all_ok = !bar_or(bar_id, n * 32, !ok);
     if (warp == lead && t.lane == 0 && all_ok) {
       if (w2 >= tc0 && w2 < tc0 + BN) st_release(sy.srv_flag + par, s2);
       if (w1 >= tc0 && w1 < tc0 + BN) st_release(sy.srv2_flag + par, s2);
@@ -551,12 +568,16 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
     }
   };
   // every piece of later steps this warp holds after the update of step
-  // s1 - 1; at a slice start (kernel start or after the slice assembly) also
-  // the rows J_{s1} and the first pivot block
+  // s1 - 1: the server blocks of step s1 + 2, the pivot columns of s1, the
+  // rows J_{s1+1}; at a slice start (kernel start or after the slice
+  // assembly) also the server blocks of step s1 + 1, the rows J_{s1} and the
+  // first pivot block
   auto publish = [&](int s1, bool slice_start) {
-    const bool next_in_slice = (s1 % p.NB) + 1 < p.NB;  // step s1 + 1 is in the same slice
+    const int k1 = s1 % p.NB;
+    const bool next_in_slice = k1 + 1 < p.NB;  // step s1 + 1 is in the same slice
     if (slice_start && in_set(kSetDjj, warp, s1)) publish_djj(s1);
-    if (next_in_slice && in_set(kSetSrv, warp, s1)) publish_srv(s1);
+    if (slice_start && next_in_slice && in_set(kSetSrv, warp, s1)) publish_srv(s1, kBarSrv);
+    if (k1 + 2 < p.NB && in_set(kSetSrv, warp, s1 + 1)) publish_srv(s1 + 1, kBarSrv2);
     if (in_set(kSetPc, warp, s1)) publish_pc(s1);
     if (slice_start && in_set(kSetPre, warp, s1)) publish_pre(s1, kBarPre0);
     if (next_in_slice && in_set(kSetPre, warp, s1 + 1)) publish_pre(s1 + 1, kBarPre1);
@@ -1019,10 +1040,10 @@ __device__ __forceinline__ void blk_gemm(const Blk& A, const Blk& B, const Blk* 
 // the 8 math warps of the server CTA form and invert every pivot block one
 // step ahead of the bulk update.  For step s (not the first of its slice):
 //   a3 = W^{(s-2)}(J_{s-1}, J_s)  = pivot rows of step s-1 (panels), columns J_s
-//   a1 = W^{(s-2)}(J_s, J_s)      } from srvbuf, published first by the math
-//   a2 = W^{(s-2)}(J_s, J_{s-1})  } warps after the update of step s-2
-// and W^{(s-1)}(J_s, J_s) = a1 - a2 (T_{s-1} a3); the product V = T_{s-1} a3
-// is formed while a1 and a2 are awaited.  The pivot rows of step s-1 stay
+//   y0 = W^{(s-2)}(J_s, J_s)      } formed by the prep warps of this CTA
+//   y1 = W^{(s-2)}(J_s, J_{s-1})  }
+// and W^{(s-1)}(J_s, J_s) = y0 - y1 (T_{s-1} a3); the product V = T_{s-1} a3
+// is formed while y0 and y1 are awaited.  The pivot rows of step s-1 stay
 // valid until the panels write those of step s+1, which needs T_s.
 template <int BM, int BN>
 __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, int t) {
@@ -1034,7 +1055,12 @@ __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, 
     const int k = s % p.NB;
     const int jn = min(kPB, p.N - k * kPB);
     const int par = s & 1;
-    if (t == 0) trace_ev(p, s, kTrPanelStart);
+    // thread 0: is the T buffer of this parity already free (read by every panel)?
+    bool tcons_ok = true;
+    if (t == 0) {
+      trace_ev(p, s, kTrPanelStart);
+      tcons_ok = s < 2 || ld_acquire(sy.t_cons + par) >= ntiles * (s >> 1);
+    }
     if (k != 0) {
       const int w = k * kPB, C2 = w / BN;
       if (warp == 0) {  // a3 comes in shares from the TR panels of its tile column
@@ -1059,54 +1085,28 @@ __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, 
       blk_gemm(sh.srv.tprev, sh.srv.a3, nullptr, 1.0, sh.srv.v, t);
     }
     if (t == 0) {
-      sh.panel_abort = k == 0 ? !wait_ge(p, sy.d_flag, s)
-                              : !(wait_ge(p, sy.srv_flag + par, s) && wait_ge(p, sy.srv2_flag + par, s));
+      sh.panel_abort = !wait_cta_ge(p, &sh.ysig[par], s);
       trace_ev(p, s, kTrPanelTin);
-    }
-    bar_sync(kBarMath, kServerThreads);
-    if (sh.panel_abort) return;
-    if (k == 0) {
-      double2 v1[kPer];
-#pragma unroll
-      for (int u = 0; u < kPer; u++) v1[u] = __ldcg(p.djjbuf + t + u * kServerThreads);
-#pragma unroll
-      for (int u = 0; u < kPer; u++) sh.srv.a1[(t + u * kServerThreads) / kPB][(t + u * kServerThreads) % kPB] = v1[u];
-    } else {
-      const double2* sb = p.srvbuf + (size_t)par * 2 * kPB * kPB;
-      double2 v1[kPer], v2[kPer];
-#pragma unroll
-      for (int u = 0; u < kPer; u++) {  // all loads in flight before the first use
-        const int e = t + u * kServerThreads;
-        v1[u] = __ldcg(sb + e);
-        v2[u] = __ldcg(sb + kPB * kPB + e);
-      }
-#pragma unroll
-      for (int u = 0; u < kPer; u++) {
-        const int e = t + u * kServerThreads, r = e / kPB, c = e % kPB;
-        sh.srv.a1[r][c] = v1[u];
-        sh.srv.a2[r][c] = v2[u];
-      }
     }
     if (t < kPB) sh.gflag[t] = 0;
     if (t == 0) sh.gj_fail = 0;
     bar_sync(kBarMath, kServerThreads);
-    if (t == 0) {
-      if (k == 0) st_release(sy.d_used, s);
-      atomicAdd(sy.srv_cons + par, 1);
-      trace_ev(p, s, kTrSrvLoaded);
-    }
-    if (k != 0) {  // W^{(s-1)}(J_s,J_s) = a1 - a2 V
-      blk_gemm(sh.srv.a2, sh.srv.v, &sh.srv.a1, -1.0, sh.srv.a1, t);
+    if (sh.panel_abort) return;
+    if (t == 0) trace_ev(p, s, kTrSrvLoaded);
+    if (k != 0) {  // W^{(s-1)}(J_s,J_s) = y0 - y1 V
+      blk_gemm(sh.srv.y[par][1], sh.srv.v, &sh.srv.y[par][0], -1.0, sh.srv.a1, t);
       bar_sync(kBarMath, kServerThreads);
     }
     if (t == 0) trace_ev(p, s, kTrSrvSchur);
     double2 a[4];
+    const Blk& a0 = (k != 0) ? sh.srv.a1 : sh.srv.y[par][0];
 #pragma unroll
-    for (int c = 0; c < 4; c++) a[c] = sh.srv.a1[lane][warp * 4 + c];
+    for (int c = 0; c < 4; c++) a[c] = a0[lane][warp * 4 + c];
     if (!gj_ahead(p, sh, a, t)) sh.gj_fail = 1;
     if (t == 0) {
       trace_ev(p, s, kTrSrvGJ);
-      sh.panel_abort = (s >= 2) ? !wait_ge(p, sy.t_cons + par, ntiles * (s >> 1)) : 0;
+      sh.panel_abort = tcons_ok ? 0 : !wait_ge(p, sy.t_cons + par, ntiles * (s >> 1));
+      st_release_cta(&sh.ycons, s);  // y[par] was read before the Gauss-Jordan started
     }
     bar_sync(kBarMath, kServerThreads);
     if (sh.panel_abort || sh.gj_fail) return;
@@ -1126,6 +1126,130 @@ __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, 
   }
 }
 
+// T-server CTA, prep warpgroup: for every step x the blocks
+//   y0 = W^{(x-2)}(J_x, J_x),  y1 = W^{(x-2)}(J_x, J_{x-1})
+// the Schur update of step x starts from.  For the second step of a slice
+// they are the blocks the math warps published after the slice assembly;
+// from the third step on the published blocks are W^{(x-3)} and get the
+// update of step x-2 here,  y = B + Pc_{x-2}(J_x, :) U_{x-2}(:, J_x or J_{x-1}),
+// from the pivot columns and U rows of step x-2 as stored for the math
+// warps.  The first step of a slice takes the first pivot block.  The math
+// pass of step x-2 is thus off the server's chain.
+template <int BM, int BN>
+__device__ void prep_role(const PersistParams& p, Shared& sh, const Sync& sy) {
+  const int t = threadIdx.x - Cfg<BM, BN>::MathThreads;
+  const int lane = t & 31, warp = t >> 5;
+  const int S = p.L * p.NB;
+  constexpr int kPer = kPB * kPB / kPanelThreads;
+  const int r = warp * 8 + (lane >> 2);  // warp w updates rows [8w, 8w+8)
+  // C += sh.T * sh.Mr on the FP64 tensor cores
+  auto gemm_acc = [&](Blk& C) {
+    for (int nt = 0; nt < kPB / 8; nt++) {
+      double acc[4];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const double2 c0 = C[r][nt * 8 + (lane & 3) * 2 + h];
+        acc[h] = c0.x;
+        acc[2 + h] = c0.y;
+      }
+#pragma unroll
+      for (int kk = 0; kk < kPB / 4; kk++) {
+        const double2 a = sh.T[r][kk * 4 + (lane & 3)];
+        const double2 bb = sh.Mr[kk * 4 + (lane & 3)][nt * 8 + (lane >> 2)];
+        dmma(acc[0], acc[1], a.x, bb.x);
+        dmma(acc[2], acc[3], a.x, bb.y);
+        dmma(acc[0], acc[1], -a.y, bb.y);
+        dmma(acc[2], acc[3], a.y, bb.x);
+      }
+#pragma unroll
+      for (int h = 0; h < 2; h++) C[r][nt * 8 + (lane & 3) * 2 + h] = cmk(acc[h], acc[2 + h]);
+    }
+  };
+  // columns [c0, c0 + 32) of U_{x-2} (zero from column lim on) -> sh.Mr
+  auto load_u = [&](const double2* ub, int c0, int lim) {
+    double2 v[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; u++) {
+      const int e = t + u * kPanelThreads, q = e / kPB, c = e % kPB;
+      v[u] = c < lim ? __ldcg(ub + swzB<BN>(q, c0 + c)) : cmk(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < kPer; u++) sh.Mr[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
+  };
+  for (int x = 0; x < S; x++) {
+    const int k = x % p.NB, par = x & 1;
+    const int w = k * kPB, jn = min(kPB, p.N - w);
+    if (warp == 0) {
+      int ok = 1;
+      if (lane == 0) {
+        trace_ev(p, x, kTrMathStart);
+        if (x >= 2) ok = wait_cta_ge(p, &sh.ycons, x - 2);  // the server has read y[par] of step x-2
+        if (ok) {
+          ok = (k == 0) ? wait_ge(p, sy.d_flag, x)
+                        : (wait_ge(p, sy.srv_flag + par, x) && wait_ge(p, sy.srv2_flag + par, x));
+        }
+        if (ok && k >= 2) ok = wait_ge(p, sy.pc_flag + w / BM, x - 2);
+      }
+      ok = __shfl_sync(kFull, ok, 0);
+      if (ok && k >= 2) {  // U_{x-2} of the tile columns holding J_x and J_{x-1}
+        ok = warp_wait_all(p, sy.u_flag + (w / BN) * p.TR, p.TR, nullptr, x - 2);
+        if (ok) ok = warp_wait_all(p, sy.u_flag + ((w - kPB) / BN) * p.TR, p.TR, nullptr, x - 2);
+      }
+      if (lane == 0) sh.prep_abort = !ok;
+    }
+    bar_sync(kBarPanel, kPanelThreads);
+    if (sh.prep_abort) return;
+    Blk& y0 = sh.srv.y[par][0];
+    Blk& y1 = sh.srv.y[par][1];
+    {
+      const double2* src = (k == 0) ? p.djjbuf : p.srvbuf + (size_t)par * 2 * kPB * kPB;
+      double2 v[kPer];
+#pragma unroll
+      for (int u = 0; u < kPer; u++) v[u] = __ldcg(src + t + u * kPanelThreads);
+#pragma unroll
+      for (int u = 0; u < kPer; u++) y0[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
+      if (k != 0) {
+#pragma unroll
+        for (int u = 0; u < kPer; u++) v[u] = __ldcg(src + kPB * kPB + t + u * kPanelThreads);
+#pragma unroll
+        for (int u = 0; u < kPer; u++) y1[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
+      }
+    }
+    if (k >= 2) {
+      // Pc_{x-2}(J_x, :), rows beyond jn zero -> sh.T; U_{x-2}(:, J_x) -> sh.Mr
+      const int I1 = w / BM;
+      const double2* pcb = p.pcbuf + ((size_t)par * p.TR + I1) * (BM * kPB) + (size_t)(w - I1 * BM) * kPB;
+      double2 v[kPer];
+#pragma unroll
+      for (int u = 0; u < kPer; u++) {
+        const int e = t + u * kPanelThreads, q = e / kPB, c = e % kPB;
+        v[u] = q < jn ? __ldcg(pcb + q * kPB + (c ^ ((q & 1) << 2))) : cmk(0.0, 0.0);
+      }
+#pragma unroll
+      for (int u = 0; u < kPer; u++) sh.T[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
+      const int C0 = w / BN;
+      load_u(p.ubuf + ((size_t)par * p.TC + C0) * (kPB * BN), w - C0 * BN, jn);
+    }
+    bar_sync(kBarPanel, kPanelThreads);
+    if (k >= 2) {
+      gemm_acc(y0);
+      bar_sync(kBarPanel, kPanelThreads);
+      const int C1 = (w - kPB) / BN;
+      load_u(p.ubuf + ((size_t)par * p.TC + C1) * (kPB * BN), w - kPB - C1 * BN, kPB);
+      bar_sync(kBarPanel, kPanelThreads);
+      gemm_acc(y1);
+      bar_sync(kBarPanel, kPanelThreads);
+    }
+    if (t == 0) {
+      if (k == 0) st_release(sy.d_used, x);
+      atomicAdd(sy.srv_cons + par, 1);
+      if (x >= 2) atomicAdd(sy.pcp_cons + par, 1);  // done with the pivot columns of step x-2
+      st_release_cta(&sh.ysig[par], x);
+      trace_ev(p, x, kTrMathDone);
+    }
+  }
+}
+
 template <int BM, int BN>
 __global__ void __launch_bounds__(Cfg<BM, BN>::Threads, 1) k_persist(PersistParams p) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -1136,6 +1260,9 @@ __global__ void __launch_bounds__(Cfg<BM, BN>::Threads, 1) k_persist(PersistPara
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&sh.mbar)) : "memory");
     sh.math_abort = 0;
     sh.panel_abort = 0;
+    sh.ysig[0] = sh.ysig[1] = -1;
+    sh.ycons = -1;
+    sh.prep_abort = 0;
   }
   __syncthreads();
   const bool server = blockIdx.x == (unsigned)(p.TR * p.TC);
@@ -1146,7 +1273,8 @@ __global__ void __launch_bounds__(Cfg<BM, BN>::Threads, 1) k_persist(PersistPara
     else math_role<BM, BN>(p, sh, sy, I, Cq);
   } else {
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(Cfg<BM, BN>::PanelRegs));
-    if (!server) panel_role<BM, BN>(p, sh, sy, I, Cq);
+    if (server) prep_role<BM, BN>(p, sh, sy);
+    else panel_role<BM, BN>(p, sh, sy, I, Cq);
   }
 }
 
