@@ -142,10 +142,11 @@ struct Shared {
       alignas(128) double2 A[kMaxTile * kPB];
       alignas(128) double2 B[kPB * kMaxTile];
     } op;
-    struct {  // T-server CTA: next pivot block, a3, T_{s-1}, scratch, and per
-              // step parity the blocks (J_s, J_s), (J_s, J_{s-1}) formed by
-              // the prep warps
-      Blk a1, a3, tprev, v;
+    struct {  // T-server CTA: next pivot block, T_{s-1}, scratch, per step
+              // parity the blocks a3 and (J_s, J_s), (J_s, J_{s-1}) staged by
+              // the prep warps, and a prep operand
+      Blk a1, tprev, v;
+      Blk a3[2];
       Blk y[2][2];
     } srv;
   };
@@ -161,9 +162,9 @@ struct Shared {
   int gflag[kPB];
   double2 drow[kPB];
   int gj_fail;  // a Gauss-Jordan wait gave up
+  int asig[2];  // T-server: step whose a3[parity] block is staged (prep -> server)
   int ysig[2];  // T-server: step whose y[parity] blocks are ready (prep -> server)
   int ycons;    // T-server: last step whose y blocks the server has read
-  int prep_abort;  // T-server CTA, prep warps: a wait gave up
   int perm[kPB], pinv[kPB];
 };
 
@@ -227,7 +228,7 @@ __device__ bool warp_wait_all(const PersistParams& p, const int* flags, int coun
 // is kept per step parity: the same-parity value can only advance after the
 // server consumed the previous one, so "flag >= s" means "published for s".
 struct Sync {
-  int *pc_flag, *pre_flag, *t_flag, *u_flag, *d_flag, *srv_flag, *d_used, *rowp_flag, *srv2_flag;
+  int *pc_flag, *pre_flag, *t_flag, *u_flag, *d_flag, *srv_flag, *d_used, *rowp_flag, *srv2_flag, *y_flag, *y_used;
   int *pc_cons, *pre_cons, *t_cons, *u_cons, *srv_cons, *pcp_cons;
   __device__ explicit Sync(const PersistParams& p) {
     pc_flag = p.flags;
@@ -239,6 +240,8 @@ struct Sync {
     d_used = srv_flag + 2;
     rowp_flag = d_used + 1;  // [TC][TR]: rows of the step in panel I's share of tile column Cq
     srv2_flag = rowp_flag + p.TR * p.TC;  // [2]: block (J_s2, J_s1), possibly from another tile column
+    y_flag = srv2_flag + 2;               // [2]: ybuf of a step parity written (prep CTA)
+    y_used = y_flag + 2;                  // last step whose ybuf the T-server CTA has loaded
     pc_cons = p.cons;
     pre_cons = pc_cons + 2 * p.TR;
     t_cons = pre_cons + 2 * p.TC;
@@ -478,7 +481,7 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
     int ok = 1;
     if (t.lane == 0 && s1 >= 2) {  // the math warps and every panel are done with step s1-2's
       ok = wait_ge(p, sy.pc_cons + par * p.TR + I, p.TC * (s1 >> 1));
-      ok = ok && wait_ge(p, sy.pcp_cons + par, (p.TR * p.TC + 1) * (s1 >> 1));
+      ok = ok && wait_ge(p, sy.pcp_cons + par, (p.TR * p.TC + 1) * (s1 >> 1));  // panels + prep CTA
     }
     ok = __shfl_sync(kFull, ok, 0);
     if (ok) {
@@ -1039,18 +1042,16 @@ __device__ __forceinline__ void blk_gemm(const Blk& A, const Blk& B, const Blk* 
 
 // the 8 math warps of the server CTA form and invert every pivot block one
 // step ahead of the bulk update.  For step s (not the first of its slice):
-//   a3 = W^{(s-2)}(J_{s-1}, J_s)  = pivot rows of step s-1 (panels), columns J_s
-//   y0 = W^{(s-2)}(J_s, J_s)      } formed by the prep warps of this CTA
-//   y1 = W^{(s-2)}(J_s, J_{s-1})  }
+//   a3 = W^{(s-2)}(J_{s-1}, J_s)  = pivot rows of step s-1, columns J_s  } staged by the
+//   y0 = W^{(s-2)}(J_s, J_s)                                             } prep warps of
+//   y1 = W^{(s-2)}(J_s, J_{s-1})                                         } this CTA
 // and W^{(s-1)}(J_s, J_s) = y0 - y1 (T_{s-1} a3); the product V = T_{s-1} a3
-// is formed while y0 and y1 are awaited.  The pivot rows of step s-1 stay
-// valid until the panels write those of step s+1, which needs T_s.
+// is formed while the prep warps finish y0 and y1.
 template <int BM, int BN>
 __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, int t) {
   const int lane = t & 31, warp = t >> 5;
   const int S = p.L * p.NB;
   const int ntiles = p.TR * p.TC;
-  constexpr int kPer = kPB * kPB / kServerThreads;
   for (int s = 0; s < S; s++) {
     const int k = s % p.NB;
     const int jn = min(kPB, p.N - k * kPB);
@@ -1061,37 +1062,18 @@ __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, 
       trace_ev(p, s, kTrPanelStart);
       tcons_ok = s < 2 || ld_acquire(sy.t_cons + par) >= ntiles * (s >> 1);
     }
-    if (k != 0) {
-      const int w = k * kPB, C2 = w / BN;
-      if (warp == 0) {  // a3 comes in shares from the TR panels of its tile column
-        const bool ok = warp_wait_all(p, sy.rowp_flag + C2 * p.TR, p.TR, nullptr, s - 1);
-        if (lane == 0) sh.panel_abort = !ok;
-      }
-      bar_sync(kBarMath, kServerThreads);
-      if (sh.panel_abort) return;
-      const double2* rwb = p.rowbuf + ((size_t)(par ^ 1) * p.TC + C2) * (kPB * BN) + (w - C2 * BN);
-      double2 v3[kPer];
-#pragma unroll
-      for (int u = 0; u < kPer; u++) {
-        const int e = t + u * kServerThreads;
-        v3[u] = __ldcg(rwb + (e / kPB) * BN + e % kPB);
-      }
-#pragma unroll
-      for (int u = 0; u < kPer; u++) {
-        const int e = t + u * kServerThreads, r = e / kPB, c = e % kPB;
-        sh.srv.a3[r][c] = c < jn ? v3[u] : cmk(0.0, 0.0);
-      }
-      bar_sync(kBarMath, kServerThreads);
-      blk_gemm(sh.srv.tprev, sh.srv.a3, nullptr, 1.0, sh.srv.v, t);
+    if (k != 0) {  // V = T_{s-1} a3 while y0 and y1 are formed
+      if (bar_or(kBarMath, kServerThreads, (t == 0) ? !wait_cta_ge(p, &sh.asig[par], s) : 0)) return;
+      blk_gemm(sh.srv.tprev, sh.srv.a3[par], nullptr, 1.0, sh.srv.v, t);
     }
+    int bad = 0;
     if (t == 0) {
-      sh.panel_abort = !wait_cta_ge(p, &sh.ysig[par], s);
+      bad = !wait_cta_ge(p, &sh.ysig[par], s);
       trace_ev(p, s, kTrPanelTin);
     }
     if (t < kPB) sh.gflag[t] = 0;
     if (t == 0) sh.gj_fail = 0;
-    bar_sync(kBarMath, kServerThreads);
-    if (sh.panel_abort) return;
+    if (bar_or(kBarMath, kServerThreads, bad)) return;
     if (t == 0) trace_ev(p, s, kTrSrvLoaded);
     if (k != 0) {  // W^{(s-1)}(J_s,J_s) = y0 - y1 V
       blk_gemm(sh.srv.y[par][1], sh.srv.v, &sh.srv.y[par][0], -1.0, sh.srv.a1, t);
@@ -1126,56 +1108,39 @@ __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, 
   }
 }
 
-// T-server CTA, prep warpgroup: for every step x the blocks
+// ---------------------------------------------------------------------------
+// prep CTA (math warpgroups): for every step x the blocks
 //   y0 = W^{(x-2)}(J_x, J_x),  y1 = W^{(x-2)}(J_x, J_{x-1})
-// the Schur update of step x starts from.  For the second step of a slice
-// they are the blocks the math warps published after the slice assembly;
-// from the third step on the published blocks are W^{(x-3)} and get the
-// update of step x-2 here,  y = B + Pc_{x-2}(J_x, :) U_{x-2}(:, J_x or J_{x-1}),
+// the T-server's Schur update of step x starts from, into ybuf[x & 1].  For
+// the second step of a slice they are the blocks the math warps published
+// after the slice assembly; from the third step on the published blocks are
+// W^{(x-3)} and get the update of step x-2 here,
+//   y = B + Pc_{x-2}(J_x, :) U_{x-2}(:, J_x or J_{x-1}),
 // from the pivot columns and U rows of step x-2 as stored for the math
-// warps.  The first step of a slice takes the first pivot block.  The math
-// pass of step x-2 is thus off the server's chain.
+// warps.  The first step of a slice passes the first pivot block on.  This
+// keeps the math pass of step x-2 off the server's chain, and the products
+// off the server's SM, whose Gauss-Jordan they would slow down.
+// ---------------------------------------------------------------------------
 template <int BM, int BN>
-__device__ void prep_role(const PersistParams& p, Shared& sh, const Sync& sy) {
-  const int t = threadIdx.x - Cfg<BM, BN>::MathThreads;
+__device__ void yprep_role(const PersistParams& p, Shared& sh, const Sync& sy, int t) {
   const int lane = t & 31, warp = t >> 5;
   const int S = p.L * p.NB;
-  constexpr int kPer = kPB * kPB / kPanelThreads;
-  const int r = warp * 8 + (lane >> 2);  // warp w updates rows [8w, 8w+8)
-  // C += sh.T * sh.Mr on the FP64 tensor cores
-  auto gemm_acc = [&](Blk& C) {
-    for (int nt = 0; nt < kPB / 8; nt++) {
-      double acc[4];
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const double2 c0 = C[r][nt * 8 + (lane & 3) * 2 + h];
-        acc[h] = c0.x;
-        acc[2 + h] = c0.y;
-      }
-#pragma unroll
-      for (int kk = 0; kk < kPB / 4; kk++) {
-        const double2 a = sh.T[r][kk * 4 + (lane & 3)];
-        const double2 bb = sh.Mr[kk * 4 + (lane & 3)][nt * 8 + (lane >> 2)];
-        dmma(acc[0], acc[1], a.x, bb.x);
-        dmma(acc[2], acc[3], a.x, bb.y);
-        dmma(acc[0], acc[1], -a.y, bb.y);
-        dmma(acc[2], acc[3], a.y, bb.x);
-      }
-#pragma unroll
-      for (int h = 0; h < 2; h++) C[r][nt * 8 + (lane & 3) * 2 + h] = cmk(acc[h], acc[2 + h]);
-    }
-  };
-  // columns [c0, c0 + 32) of U_{x-2} (zero from column lim on) -> sh.Mr
-  auto load_u = [&](const double2* ub, int c0, int lim) {
+  constexpr int kPer = kPB * kPB / kServerThreads;
+  // bounded load of a 32x32 block (row stride ld; entries outside rows x cols
+  // zero; column c read at col_of(c)) into a padded shared block
+  auto load_blk = [&](Blk& dst, const double2* src, int ld, int rows, int cols, auto col_of) {
     double2 v[kPer];
 #pragma unroll
     for (int u = 0; u < kPer; u++) {
-      const int e = t + u * kPanelThreads, q = e / kPB, c = e % kPB;
-      v[u] = c < lim ? __ldcg(ub + swzB<BN>(q, c0 + c)) : cmk(0.0, 0.0);
+      const int e = t + u * kServerThreads, q = e / kPB, c = e % kPB;
+      v[u] = (q < rows && c < cols) ? __ldcg(src + (size_t)q * ld + col_of(q, c)) : cmk(0.0, 0.0);
     }
 #pragma unroll
-    for (int u = 0; u < kPer; u++) sh.Mr[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
+    for (int u = 0; u < kPer; u++) dst[(t + u * kServerThreads) / kPB][(t + u * kServerThreads) % kPB] = v[u];
   };
+  auto plain = [](int, int c) { return c; };
+  Blk& y0 = sh.srv.y[0][0];
+  Blk& y1 = sh.srv.y[0][1];
   for (int x = 0; x < S; x++) {
     const int k = x % p.NB, par = x & 1;
     const int w = k * kPB, jn = min(kPB, p.N - w);
@@ -1183,7 +1148,7 @@ __device__ void prep_role(const PersistParams& p, Shared& sh, const Sync& sy) {
       int ok = 1;
       if (lane == 0) {
         trace_ev(p, x, kTrMathStart);
-        if (x >= 2) ok = wait_cta_ge(p, &sh.ycons, x - 2);  // the server has read y[par] of step x-2
+        if (x >= 2) ok = wait_ge(p, sy.y_used, x - 2);  // ybuf[par] of step x-2 was loaded
         if (ok) {
           ok = (k == 0) ? wait_ge(p, sy.d_flag, x)
                         : (wait_ge(p, sy.srv_flag + par, x) && wait_ge(p, sy.srv2_flag + par, x));
@@ -1195,57 +1160,99 @@ __device__ void prep_role(const PersistParams& p, Shared& sh, const Sync& sy) {
         ok = warp_wait_all(p, sy.u_flag + (w / BN) * p.TR, p.TR, nullptr, x - 2);
         if (ok) ok = warp_wait_all(p, sy.u_flag + ((w - kPB) / BN) * p.TR, p.TR, nullptr, x - 2);
       }
-      if (lane == 0) sh.prep_abort = !ok;
+      sh.panel_abort = !ok;  // every lane writes the same value
     }
-    bar_sync(kBarPanel, kPanelThreads);
-    if (sh.prep_abort) return;
-    Blk& y0 = sh.srv.y[par][0];
-    Blk& y1 = sh.srv.y[par][1];
-    {
-      const double2* src = (k == 0) ? p.djjbuf : p.srvbuf + (size_t)par * 2 * kPB * kPB;
-      double2 v[kPer];
-#pragma unroll
-      for (int u = 0; u < kPer; u++) v[u] = __ldcg(src + t + u * kPanelThreads);
-#pragma unroll
-      for (int u = 0; u < kPer; u++) y0[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
-      if (k != 0) {
-#pragma unroll
-        for (int u = 0; u < kPer; u++) v[u] = __ldcg(src + kPB * kPB + t + u * kPanelThreads);
-#pragma unroll
-        for (int u = 0; u < kPer; u++) y1[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
-      }
+    bar_sync(kBarMath, kServerThreads);
+    if (sh.panel_abort) return;
+    if (k == 0) {
+      load_blk(y0, p.djjbuf, kPB, kPB, kPB, plain);
+    } else {
+      const double2* sb = p.srvbuf + (size_t)par * 2 * kPB * kPB;
+      load_blk(y0, sb, kPB, kPB, kPB, plain);
+      load_blk(y1, sb + kPB * kPB, kPB, kPB, kPB, plain);
     }
     if (k >= 2) {
-      // Pc_{x-2}(J_x, :), rows beyond jn zero -> sh.T; U_{x-2}(:, J_x) -> sh.Mr
-      const int I1 = w / BM;
-      const double2* pcb = p.pcbuf + ((size_t)par * p.TR + I1) * (BM * kPB) + (size_t)(w - I1 * BM) * kPB;
-      double2 v[kPer];
-#pragma unroll
-      for (int u = 0; u < kPer; u++) {
-        const int e = t + u * kPanelThreads, q = e / kPB, c = e % kPB;
-        v[u] = q < jn ? __ldcg(pcb + q * kPB + (c ^ ((q & 1) << 2))) : cmk(0.0, 0.0);
-      }
-#pragma unroll
-      for (int u = 0; u < kPer; u++) sh.T[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
-      const int C0 = w / BN;
-      load_u(p.ubuf + ((size_t)par * p.TC + C0) * (kPB * BN), w - C0 * BN, jn);
+      // Pc_{x-2}(J_x, :), rows beyond jn zero -> sh.T; U_{x-2}(:, J_x), columns
+      // beyond jn zero -> sh.Mr; U_{x-2}(:, J_{x-1}) -> srv.v
+      const int I1 = w / BM, C0 = w / BN, C1 = (w - kPB) / BN;
+      load_blk(sh.T, p.pcbuf + ((size_t)par * p.TR + I1) * (BM * kPB) + (size_t)(w - I1 * BM) * kPB, kPB, jn, kPB,
+               [](int q, int c) { return c ^ ((q & 1) << 2); });
+      const int o0 = w - C0 * BN, o1 = w - kPB - C1 * BN;
+      load_blk(sh.Mr, p.ubuf + ((size_t)par * p.TC + C0) * (kPB * BN), 0, kPB, jn,
+               [o0](int q, int c) { return swzB<BN>(q, o0 + c); });
+      load_blk(sh.srv.v, p.ubuf + ((size_t)par * p.TC + C1) * (kPB * BN), 0, kPB, kPB,
+               [o1](int q, int c) { return swzB<BN>(q, o1 + c); });
     }
-    bar_sync(kBarPanel, kPanelThreads);
-    if (k >= 2) {
-      gemm_acc(y0);
-      bar_sync(kBarPanel, kPanelThreads);
-      const int C1 = (w - kPB) / BN;
-      load_u(p.ubuf + ((size_t)par * p.TC + C1) * (kPB * BN), w - kPB - C1 * BN, kPB);
-      bar_sync(kBarPanel, kPanelThreads);
-      gemm_acc(y1);
-      bar_sync(kBarPanel, kPanelThreads);
-    }
-    if (t == 0) {
+    bar_sync(kBarMath, kServerThreads);
+    if (t == 0) {  // every input is in shared memory: its buffers may be reused
       if (k == 0) st_release(sy.d_used, x);
       atomicAdd(sy.srv_cons + par, 1);
       if (x >= 2) atomicAdd(sy.pcp_cons + par, 1);  // done with the pivot columns of step x-2
-      st_release_cta(&sh.ysig[par], x);
+    }
+    if (k >= 2) {  // the update by step x-2
+      blk_gemm(sh.T, sh.Mr, &y0, 1.0, y0, t);
+      blk_gemm(sh.T, sh.srv.v, &y1, 1.0, y1, t);
+      bar_sync(kBarMath, kServerThreads);
+    }
+    double2* yb = p.ybuf + (size_t)par * 2 * kPB * kPB;
+#pragma unroll
+    for (int u = 0; u < kPer; u++) {
+      const int e = t + u * kServerThreads;
+      __stcg(yb + e, y0[e / kPB][e % kPB]);
+      if (k != 0) __stcg(yb + kPB * kPB + e, y1[e / kPB][e % kPB]);
+    }
+    bar_sync(kBarMath, kServerThreads);
+    if (t == 0) {
+      st_release(sy.y_flag + par, x);
       trace_ev(p, x, kTrMathDone);
+    }
+  }
+}
+
+// T-server CTA, stage warpgroup: copies each step's a3 (the pivot rows of
+// step x-1 in columns J_x, from the panels) and y blocks (from the prep CTA)
+// into shared memory ahead of the server warps, which find them there.
+template <int BM, int BN>
+__device__ void stage_role(const PersistParams& p, Shared& sh, const Sync& sy) {
+  const int t = threadIdx.x - Cfg<BM, BN>::MathThreads;
+  const int lane = t & 31, warp = t >> 5;
+  const int S = p.L * p.NB;
+  constexpr int kPer = kPB * kPB / kPanelThreads;
+  auto copy_blk = [&](Blk& dst, const double2* src, int ld, int cols) {
+    double2 v[kPer];
+#pragma unroll
+    for (int u = 0; u < kPer; u++) {
+      const int e = t + u * kPanelThreads, q = e / kPB, c = e % kPB;
+      v[u] = c < cols ? __ldcg(src + (size_t)q * ld + c) : cmk(0.0, 0.0);
+    }
+#pragma unroll
+    for (int u = 0; u < kPer; u++) dst[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
+  };
+  for (int x = 0; x < S; x++) {
+    const int k = x % p.NB, par = x & 1;
+    const int w = k * kPB, jn = min(kPB, p.N - w);
+    // the server warps are done with [par] of step x-2
+    if (x >= 2 && bar_or(kBarPanel, kPanelThreads, (t == 0) ? !wait_cta_ge(p, &sh.ycons, x - 2) : 0)) return;
+    if (k != 0) {  // a3 comes in shares from the TR panels of its tile column
+      int bad = 0;
+      if (warp == 0) {
+        const bool ok = warp_wait_all(p, sy.rowp_flag + (w / BN) * p.TR, p.TR, nullptr, x - 1);
+        bad = (lane == 0) && !ok;
+      }
+      if (bar_or(kBarPanel, kPanelThreads, bad)) return;
+      const int C2 = w / BN;
+      copy_blk(sh.srv.a3[par], p.rowbuf + ((size_t)(par ^ 1) * p.TC + C2) * (kPB * BN) + (w - C2 * BN), BN, jn);
+      bar_sync(kBarPanel, kPanelThreads);
+      if (t == 0) st_release_cta(&sh.asig[par], x);
+    }
+    if (bar_or(kBarPanel, kPanelThreads, (t == 0) ? !wait_ge(p, sy.y_flag + par, x) : 0)) return;
+    const double2* yb = p.ybuf + (size_t)par * 2 * kPB * kPB;
+    copy_blk(sh.srv.y[par][0], yb, kPB, kPB);
+    if (k != 0) copy_blk(sh.srv.y[par][1], yb + kPB * kPB, kPB, kPB);
+    bar_sync(kBarPanel, kPanelThreads);
+    if (t == 0) {
+      st_release_cta(&sh.ysig[par], x);
+      st_release(sy.y_used, x);
     }
   }
 }
@@ -1261,20 +1268,22 @@ __global__ void __launch_bounds__(Cfg<BM, BN>::Threads, 1) k_persist(PersistPara
     sh.math_abort = 0;
     sh.panel_abort = 0;
     sh.ysig[0] = sh.ysig[1] = -1;
+    sh.asig[0] = sh.asig[1] = -1;
     sh.ycons = -1;
-    sh.prep_abort = 0;
   }
   __syncthreads();
   const bool server = blockIdx.x == (unsigned)(p.TR * p.TC);
+  const bool yprep = blockIdx.x == (unsigned)(p.TR * p.TC + 1);
   static_assert(Cfg<BM, BN>::MathThreads == kServerThreads, "the server uses the math warpgroups");
   if (threadIdx.x < Cfg<BM, BN>::MathThreads) {
     asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(Cfg<BM, BN>::MathRegs));
     if (server) server_role<BM, BN>(p, sh, sy, threadIdx.x);
+    else if (yprep) yprep_role<BM, BN>(p, sh, sy, threadIdx.x);
     else math_role<BM, BN>(p, sh, sy, I, Cq);
   } else {
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(Cfg<BM, BN>::PanelRegs));
-    if (server) prep_role<BM, BN>(p, sh, sy);
-    else panel_role<BM, BN>(p, sh, sy, I, Cq);
+    if (server) stage_role<BM, BN>(p, sh, sy);
+    else if (!yprep) panel_role<BM, BN>(p, sh, sy, I, Cq);
   }
 }
 
@@ -1289,12 +1298,12 @@ int persist_threads(int BM, int BN) {
 }
 
 // tile shape: the largest that keeps >= 60% of the SMs busy, else the one
-// with the most CTAs; one SM always stays free for the T-server CTA.  With
+// with the most CTAs; two SMs always stay free for the T-server and prep CTAs.  With
 // prefer_large (several sweeps sharing the GPU) simply the largest tile whose
 // grid fits in `sms`.
 bool persist_choose_tile(int64_t R, int64_t C, int sms, int* BM, int* BN, bool prefer_large) {
   const int cand[3] = {96, 64, 32};
-  const int avail = sms - 1;
+  const int avail = sms - kPersistExtraCtas;
   for (int q = 0; q < 3 && prefer_large; q++) {
     const int64_t tiles = ((R + cand[q] - 1) / cand[q]) * ((C + cand[q] - 1) / cand[q]);
     if (tiles <= avail) {
@@ -1330,7 +1339,8 @@ cudaError_t launch_persist(const PersistParams& p, int BM, int BN, cudaStream_t 
   else return cudaErrorInvalidValue;
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  return cudaLaunchCooperativeKernel(fn, dim3(p.TR * p.TC + 1), dim3(persist_threads(BM, BN)), args, smem, s);
+  return cudaLaunchCooperativeKernel(fn, dim3(p.TR * p.TC + kPersistExtraCtas), dim3(persist_threads(BM, BN)), args,
+                                     smem, s);
 }
 
 }  // namespace rgf

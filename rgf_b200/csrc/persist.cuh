@@ -23,8 +23,10 @@ struct PersistParams {
   double2* tbuf;         // [2][32][32]
   double2* ubuf;         // [2][TC][32][BN]
   double2* djjbuf;       // [32][32] first pivot block of a slice, for the T-server CTA
-  double2* srvbuf;       // [2][2][32][32] blocks the T-server updates into the next pivot block
-  int* flags;  // pc[TR], pre[2][TC], t[1], u[TC*TR], d[1], srv[2], d_used[1], rowp[TC*TR], srv2[2] (init -1)
+  double2* srvbuf;       // [2][2][32][32] blocks the prep CTA updates into the T-server's blocks
+  double2* ybuf;         // [2][2][32][32] the T-server's blocks (J_s, J_s), (J_s, J_{s-1}) of a step
+  int* flags;  // pc[TR], pre[2][TC], t[1], u[TC*TR], d[1], srv[2], d_used[1], rowp[TC*TR], srv2[2],
+               // y[2], y_used[1] (init -1)
   int* cons;   // pc[2][TR], pre[2][TC], t[2], u[2][TC], srv[2], pcp[2]                              (init 0)
   // optional snapshots of W after slice n (launch-relative) for every n with
   // n % snap_mod == snap_mod - 1, at snap + (n / snap_mod) * snap_ld, laid
@@ -54,7 +56,9 @@ enum { kTrMathStart = 0, kTrMathOperands, kTrMathCopied, kTrMathPublished, kTrMa
        // T-server: end of the factorization of each 4-pivot group
        kTrSrvGroup0, kTraceEvents = kTrSrvGroup0 + 8 };
 
-inline int persist_flag_words(int TR, int TC) { return TR + 2 * TC + 1 + TR * TC + 1 + 2 + 1 + TR * TC + 2; }
+inline int persist_flag_words(int TR, int TC) { return TR + 2 * TC + 1 + TR * TC + 1 + 2 + 1 + TR * TC + 2 + 3; }
+// CTAs beyond the TR x TC tiles: the T-server and the prep CTA
+constexpr int kPersistExtraCtas = 2;
 inline int persist_cons_words(int TR, int TC) { return 2 * TR + 2 * TC + 2 + 2 * TC + 2 + 2; }
 
 size_t persist_smem_bytes();

@@ -595,7 +595,7 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
       const int nflags = persist_flag_words(TR, TC), ncons = persist_cons_words(TR, TC);
       if ((st = ensure(h->xpc, sizeof(double2) * 2 * TR * BMp * 32))) return st;
       if ((st = ensure(h->xrow, sizeof(double2) * 4 * TC * 32 * BNp))) return st;  // rowbuf, prebuf
-      if ((st = ensure(h->xt, sizeof(double2) * 7 * 32 * 32))) return st;  // tbuf[2], djjbuf, srvbuf[2][2]
+      if ((st = ensure(h->xt, sizeof(double2) * 11 * 32 * 32))) return st;  // tbuf[2], djjbuf, srvbuf[2][2], ybuf[2][2]
       if ((st = ensure(h->xu, sizeof(double2) * 2 * TC * 32 * BNp))) return st;
       if ((st = ensure(h->xsync, sizeof(int) * (nflags + ncons + 4)))) return st;
       int* flags = as<int>(h->xsync);
@@ -626,6 +626,7 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
       pp.tbuf = as<double2>(h->xt);
       pp.djjbuf = as<double2>(h->xt) + 2 * 32 * 32;
       pp.srvbuf = as<double2>(h->xt) + 3 * 32 * 32;
+      pp.ybuf = as<double2>(h->xt) + 7 * 32 * 32;
       pp.ubuf = as<double2>(h->xu);
       pp.flags = flags;
       pp.cons = flags + nflags;
@@ -658,7 +659,7 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
       if (trace_path && *trace_path) {
         pp.trace_steps = steps_env ? std::max(1, std::min(atoi(steps_env), (int)(nsl * pp.NB))) : 128;
         if ((st = ensure(h->xtrace,
-                         sizeof(unsigned long long) * (size_t)(TR * TC + 1) * pp.trace_steps * kTraceEvents)))
+                         sizeof(unsigned long long) * (size_t)(TR * TC + kPersistExtraCtas) * pp.trace_steps * kTraceEvents)))
           return st;
         pp.trace = as<unsigned long long>(h->xtrace);
         RGF_CUDA_TRY(cudaMemsetAsync(pp.trace, 0, h->xtrace.bytes, h->stream));
@@ -674,7 +675,7 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
       }
       // in a batch, hold SMs for the whole cooperative grid while it runs, so
       // that the grids of concurrent pipelines always fit on the GPU together
-      const int need = TR * TC + 1;
+      const int need = TR * TC + kPersistExtraCtas;
       if (h->sm_budget) {
         for (;;) {
           int cur = h->sm_budget->load();
@@ -720,7 +721,7 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
           }
         }
         if (pp.trace) {
-          std::vector<unsigned long long> tr((size_t)(TR * TC + 1) * pp.trace_steps * kTraceEvents);
+          std::vector<unsigned long long> tr((size_t)(TR * TC + kPersistExtraCtas) * pp.trace_steps * kTraceEvents);
           cudaStream_t rd = h->stream;
           if (hung) RGF_CUDA_TRY(cudaStreamCreateWithFlags(&rd, cudaStreamNonBlocking));
           RGF_CUDA_TRY(cudaMemcpyAsync(tr.data(), pp.trace, sizeof(unsigned long long) * tr.size(),
