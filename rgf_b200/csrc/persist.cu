@@ -834,13 +834,16 @@ __device__ void panel_role(const PersistParams& p, Shared& sh, const Sync& sy, i
         for (int u = 0; u < kPer; u++) sh.Mr[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
       }
       if (t == 0) {
+        // the math warps of tile column Cq have copied U of step s-2 (checked
+        // before T_s comes, so that it costs nothing on the path from T_s)
         trace_ev(p, s, kTrPanelStart);
-        sh.panel_abort = !wait_ge(p, sy.t_flag, s);
+        int ok = (w > 0 && s >= 2) ? wait_ge(p, sy.u_cons + par * p.TC + Cq, p.TR * (s >> 1)) : 1;
+        ok = ok && wait_ge(p, sy.t_flag, s);
+        sh.panel_abort = !ok;
         trace_ev(p, s, kTrPanelUin);
       }
       bar_sync(kBarPanel, kPanelThreads);
       if (sh.panel_abort) return;
-      bool waited_u = false;
       for (int cc = 0; cc < w; cc += kPB) {
         const int wc = min(kPB, w - cc);
         if (cc == 0) {
@@ -858,12 +861,6 @@ __device__ void panel_role(const PersistParams& p, Shared& sh, const Sync& sy, i
           for (int u = 0; u < kPer; u++) sh.Mr[(t + u * kPanelThreads) / kPB][(t + u * kPanelThreads) % kPB] = v[u];
         }
         bar_sync(kBarPanel, kPanelThreads);
-        if (!waited_u) {
-          if (t == 0) sh.panel_abort = (s >= 2) ? !wait_ge(p, sy.u_cons + par * p.TC + Cq, p.TR * (s >> 1)) : 0;
-          bar_sync(kBarPanel, kPanelThreads);
-          if (sh.panel_abort) return;
-          waited_u = true;
-        }
         // T_s is padded with the identity and the pivot rows with zeros beyond jn
         for (int nt = 0; nt * 8 < wc; nt++) {
           double acc[4] = {0.0, 0.0, 0.0, 0.0};
