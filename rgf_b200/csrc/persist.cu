@@ -13,20 +13,26 @@
 // where W_mod is W with the rows and columns of J zeroed.  Roles:
 //  * tile CTA, 2 math warpgroups: wait for Pc(I) and U(Cq) of step s, stage
 //    them in shared memory with TMA bulk copies (cp.async.bulk + mbarrier) and
-//    update the register tile with mma.sync.m8n8k4.f64.  The subtiles holding
-//    pieces of later steps go first and are published right away: the pivot
-//    rows W(J_{s+1}, Cq) and columns W(I, J_{s+1}) of step s+1, and the
-//    32x32 block (J_{s+2},J_{s+2}) of W after step s for the T-server.
-//  * tile CTA, 1 panel warpgroup: its ceil(BN/TR)-column slice of U_s(Cq),
-//    on the FP64 tensor cores.
-//  * T-server CTA (one extra CTA on an SM of its own, so its FP64 pipe is not
-//    shared with the bulk update): one step ahead of the bulk it forms the
-//    next pivot block as the Schur update
-//        W^{(s-1)}(J_s,J_s) = W^{(s-2)}(J_s,J_s) - W^{(s-2)}(J_s,J_{s-1}) T_{s-1} W^{(s-2)}(J_{s-1},J_s)
-//    (W^{(s)} = W after step s) and inverts it by register-resident
-//    Gauss-Jordan with partial pivoting (redux.sync pivot search, implicit row
-//    interchanges, one barrier per pivot); the first pivot block of every
-//    slice comes straight from the slice assembly.
+//    update the whole register tile with mma.sync.m8n8k4.f64.  Then the warps
+//    holding them publish pieces of later steps: the blocks (J_x, J_x) and
+//    (J_x, J_{x-1}) of x = s+3 for the prep CTA, the pivot columns
+//    W(I, J_{s+1}) of step s+1, and the rows W(J_{s+2}, Cq) for the panels.
+//  * tile CTA, 1 panel warpgroup: its ceil(BN/TR)-column share of U_s(Cq)
+//    as soon as T_s is out, then one step ahead the pivot rows of step s+1
+//    in its share (the rows J_{s+1} published after step s-1, updated by
+//    step s), both on the FP64 tensor cores.
+//  * prep CTA (SM of its own): for step x, once U_{x-2} is out, the blocks
+//        y0 = W^{(x-2)}(J_x,J_x),  y1 = W^{(x-2)}(J_x,J_{x-1})
+//    (W^{(s)} = W after step s) from the blocks published after step x-3.
+//  * T-server CTA (SM of its own, so its FP64 pipe is not shared with the
+//    bulk update): its fourth warpgroup stages y0, y1 and
+//    a3 = W^{(x-2)}(J_{x-1},J_x) (from the panels' pivot rows) in shared
+//    memory; its 8 math warps form the next pivot block by the Schur update
+//        W^{(s-1)}(J_s,J_s) = y0 - y1 (T_{s-1} a3)
+//    and invert it by register-resident Gauss-Jordan with partial pivoting
+//    (owner warps run ahead with per-row release counters, redux.sync pivot
+//    search, implicit row interchanges, rows scaled once at the end); the
+//    first pivot block of every slice comes straight from the slice assembly.
 // setmaxnreg moves registers from the panel warpgroup (88) to the math
 // warpgroups (208) so the 96x96 complex tile (144 registers/thread) fits.
 // Exchange buffers are double-buffered by step parity; each has a publication
