@@ -51,11 +51,15 @@ typedef enum {
   RGF_OK = 0,
   RGF_ERR_ARG = 1,       /* invalid argument (MATLAB error() in the reference)          */
   RGF_ERR_NONFINITE = 2, /* NaN/Inf in epsilon, epsilon_L/R or k0dx                      */
-  RGF_ERR_SINGULAR = 3,  /* a pivot block of a slice matrix is singular/ill-conditioned */
+  RGF_ERR_SINGULAR = 3,  /* a slice matrix is singular (zero pivot under partial pivoting) */
   RGF_ERR_TIMEOUT = 4,   /* a device-side wait gave up (bounded spin)                    */
   RGF_ERR_CUDA = 5,      /* CUDA runtime error                                           */
   RGF_ERR_OOM = 6,       /* device allocation failed                                     */
-  RGF_ERR_NODEVICE = 7   /* no usable CUDA device                                        */
+  RGF_ERR_NODEVICE = 7,  /* no usable CUDA device                                        */
+  RGF_ERR_ILLCOND = 8    /* a slice inverse failed its a-posteriori check even under
+                            partial pivoting over the whole column (residual > 1e-8):
+                            S and channels are written but may be inaccurate (where
+                            MATLAB's inv warns "close to singular or badly scaled")  */
 } rgf_status;
 
 /* Transverse boundary conditions (setup_channels.m:10-20, build_laplacian_1d.m:9-17). */
@@ -111,8 +115,13 @@ typedef struct {
 
 typedef struct {
   int32_t precision;  /* rgf_precision (0 = RGF_FP64)                                  */
-  int32_t engine;     /* 0: persistent register-resident sweep kernel when the matrix
-                         fits on the GPU (default), 1: one launch pair per pivot step */
+  int32_t engine;     /* 0 (default): persistent register-resident sweep kernel when
+                         the matrix fits on the GPU, pivoting inside each 32 x 32
+                         pivot block; every slice inverse is checked a posteriori
+                         and the call is recomputed with engine 1 if one fails.
+                         1: one launch sequence per pivot step with partial
+                         pivoting over the whole column (LAPACK zgetrf's choice,
+                         as MATLAB's inv)                                            */
   int32_t S_on_device;/* 1: S is a device pointer (no D2H copy)                        */
   int32_t profile;    /* > 0: time the dominant kernel with CUDA events on every
                          profile-th slice (read back with rgf_last_profile)           */
@@ -181,6 +190,50 @@ RGF_API rgf_status rgf_smatrix_grad_3d(rgf_handle h, const rgf_syst3d* syst, con
                                        const rgf_options* opt, const rgf_cplx* D, int64_t ldD, rgf_cplx* S,
                                        int64_t ldS, rgf_cplx* g, int64_t checkpoint);
 
+/* Fields inside the structure (an addition: the reference computes S only and
+ * points to MESTI for fields, README.md:13).  Computes S as rgf_smatrix_2d/3d
+ * and, for every requested input channel b (the columns of S, in S's order),
+ *     psi[m + n*N + b*N*L] = (G_{n, s(b)} B_b)_m,
+ * the response at transverse site m (N = ny, or nx*ny in 3D, x fastest) of
+ * slice n (0 <= n < L = nx, or nz in 3D) to the source profile B_b of channel
+ * b on its lead's surface slice s(b) (B = phi(:, ind_prop) sqrt(mu), the
+ * matrix S = -2i C G B - delta is built from; cal_smatrix_RGF.m:191-195),
+ * i.e. column b of the block-tridiagonal Green's function times B, laid out
+ * as a MATLAB array [ny, nx, n_in] ([nx, ny, nz, n_in] in 3D).  The same
+ * backward recursion as the gradient (checkpoint as there).  At least one
+ * output channel must be requested.  psi is a device pointer when
+ * opt->S_on_device, host memory otherwise. */
+RGF_API rgf_status rgf_fields_2d(rgf_handle h, const rgf_syst2d* syst, const rgf_request* req,
+                                 const rgf_options* opt, rgf_cplx* S, int64_t ldS, rgf_cplx* psi,
+                                 int64_t checkpoint);
+RGF_API rgf_status rgf_fields_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_request* req,
+                                 const rgf_options* opt, rgf_cplx* S, int64_t ldS, rgf_cplx* psi,
+                                 int64_t checkpoint);
+
+/* L-split S-matrix (an addition: the reference's loop over slices,
+ * cal_smatrix_RGF.m:263-269, is strictly sequential).  The slices are cut at
+ * `cut` (0 < cut < L): rgf_segment_sweep_* with side = 0 sweeps [0, cut) from
+ * the left lead, with side = 1 [cut, L) from the right lead, carrying only
+ * that side's requested channels, and writes the segment state
+ *     state = [[g, X], [Z, Y]]   row-major, (N + n_out_side) x (N + n_in_side),
+ * g the lead-connected Green's function of the part's last slice, X = G B,
+ * Z = C G, Y = C G B at that lead.  The two sweeps are independent (two GPUs,
+ * or one after the other on one); rgf_segment_merge_* joins the two states
+ * across the cut by the Dyson equation of two Green's functions coupled by
+ * the hopping -I (one sweep of a matrix of order N + n_out with pivot block
+ * I - g_R g_L) and writes S as rgf_smatrix_*.  state / S are device pointers
+ * when opt->S_on_device. */
+RGF_API rgf_status rgf_segment_sweep_2d(rgf_handle h, const rgf_syst2d* syst, const rgf_request* req,
+                                        const rgf_options* opt, int32_t side, int64_t cut, rgf_cplx* state);
+RGF_API rgf_status rgf_segment_sweep_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_request* req,
+                                        const rgf_options* opt, int32_t side, int64_t cut, rgf_cplx* state);
+RGF_API rgf_status rgf_segment_merge_2d(rgf_handle h, const rgf_syst2d* syst, const rgf_request* req,
+                                        const rgf_options* opt, const rgf_cplx* state_L, const rgf_cplx* state_R,
+                                        rgf_cplx* S, int64_t ldS);
+RGF_API rgf_status rgf_segment_merge_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_request* req,
+                                        const rgf_options* opt, const rgf_cplx* state_L, const rgf_cplx* state_R,
+                                        rgf_cplx* S, int64_t ldS);
+
 /* Size of the S block a request selects (needs the channel count, so it runs
  * the channel set-up on the device). */
 RGF_API rgf_status rgf_smatrix_size_2d(rgf_handle h, const rgf_syst2d* syst, const rgf_request* req,
@@ -208,6 +261,12 @@ RGF_API const char* rgf_version(void);
  * posteriori check of every slice inverse, carried as two extra columns of
  * the swept matrix). */
 RGF_API rgf_status rgf_last_stats(rgf_handle h, int64_t* kernel_launches, double* probe_residual);
+/* Engine that produced the last rgf_smatrix_* result on this handle (0 or 1,
+ * see rgf_options.engine); fallback = 1 when the persistent engine's result
+ * was rejected by the a-posteriori check (a zero or non-finite in-block
+ * pivot, or a probe residual above 1e-10) and recomputed with engine 1;
+ * rejected_probe is that run's residual.  An addition of this library. */
+RGF_API rgf_status rgf_last_engine(rgf_handle h, int32_t* engine, int32_t* fallback, double* rejected_probe);
 /* Sampled timing of the dominant kernel of the last rgf_smatrix_* call made
  * with opt->profile > 0: number of timed launches, their summed duration (ms),
  * the algorithmic flops of one such launch, and its name. */
@@ -232,9 +291,14 @@ RGF_API rgf_status rgf_set_stream(rgf_handle h, void* stream);
  * exchange buffers and flags -- is carved from one static device array of
  * RGF_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until
  * the process exits.  A problem whose workspace does not fit is rejected with
- * RGF_ERR_ARG and a message naming the limit (roughly: 16 bytes times
- * (N + n_out)(N + n_in + 2) for the slice matrix, plus N*L*16 when epsilon is
- * on the host, plus a few N-sized arrays, N = ny).  Work is issued on
+ * RGF_ERR_ARG and a message naming the limit.  The workspace is, in bytes,
+ * with N = ny, R = N + n_out, C = N + n_in + 2 (n_out, n_in: the sizes of
+ * the requested S block):
+ *     16 * (3 N^2 + R (C + 1) + 64 R + 288 C + 110 N)      about, and
+ *   + 16 N^2      when epsilon_L != epsilon_R (a second lead),
+ *   + 16 N nx     when epsilon is in host memory (eps_on_device = 0),
+ * which puts the largest ny near 615 for the full S of a periodic problem at
+ * k0dx = 2 pi / 15 (about 2 ny / 15 channels per side).  Work is issued on
  * `stream` (a cudaStream_t; NULL = the legacy default stream) of the current
  * device.  The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call

@@ -14,9 +14,7 @@ function [smatrix, channels] = cal_smatrix_RGF(syst, out, in)
 if nargin < 3
     error('Not enough input arguments.');
 end
-if ~isstruct(syst)
-    error('syst must be a structure');
-end
+rgf_check_syst(syst, out, in, 2);
 [smatrix, channels] = rgf_mex('smatrix2d', syst, out, in);
 channels.fun_phi = rgf_fun_phi(syst.yBC, size(syst.epsilon, 1));
 end

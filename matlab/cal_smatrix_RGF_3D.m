@@ -9,9 +9,7 @@ function [smatrix, channels] = cal_smatrix_RGF_3D(syst, out, in)
 if nargin < 3
     error('Not enough input arguments.');
 end
-if ~isstruct(syst)
-    error('syst must be a structure');
-end
+rgf_check_syst(syst, out, in, 3);
 [smatrix, ch] = rgf_mex('smatrix3d', syst, out, in);
 [nx, ny, ~] = size(syst.epsilon);
 channels = rgf_channels_3d(ch, syst.xyBC, nx, ny);

@@ -13,6 +13,7 @@ function [smatrix, dF_deps] = cal_smatrix_RGF_grad(syst, out, in, D)
 if nargin < 4
     error('Not enough input arguments.');
 end
+rgf_check_syst(syst, out, in, 2);
 [smatrix, g] = rgf_mex('grad2d', syst, out, in, D);
 dF_deps = 2 * real(g);
 end

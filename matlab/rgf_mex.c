@@ -18,6 +18,7 @@
  * here and 0-based in the C ABI.  Every library status maps to a MATLAB
  * error with identifier rgf:<status> and the library's message.
  */
+#include <math.h>
 #include <stdio.h>
 #include <string.h>
 
@@ -32,13 +33,16 @@ static void at_exit(void) {
 }
 
 static void fail(rgf_status st) {
-  static const char* ids[] = {"rgf:ok",       "rgf:arg", "rgf:nonfinite", "rgf:singular",
-                              "rgf:timeout",  "rgf:cuda", "rgf:oom",      "rgf:nodevice"};
-  mexErrMsgIdAndTxt(st >= 0 && st <= 7 ? ids[st] : "rgf:error", "%s", rgf_last_error());
+  static const char* ids[] = {"rgf:ok",      "rgf:arg",  "rgf:nonfinite", "rgf:singular", "rgf:timeout",
+                              "rgf:cuda",    "rgf:oom",  "rgf:nodevice",  "rgf:illcond"};
+  mexErrMsgIdAndTxt(st >= 0 && st <= 8 ? ids[st] : "rgf:error", "%s", rgf_last_error());
 }
 
+/* RGF_ERR_ILLCOND leaves a result behind: a warning, as MATLAB's inv gives
+ * for a matrix close to singular; every other failure is an error */
 static void check(rgf_status st) {
-  if (st != RGF_OK) fail(st);
+  if (st == RGF_ERR_ILLCOND) mexWarnMsgIdAndTxt("rgf:illcond", "%s", rgf_last_error());
+  else if (st != RGF_OK) fail(st);
 }
 
 static void ensure_handle(void) {
@@ -106,8 +110,10 @@ static const rgf_cplx* eps_of(const mxArray* e, mxArray** tmp) {
   return (const rgf_cplx*)mxGetComplexDoubles(*tmp);
 }
 
-/* one side's list: NULL = not given; otherwise 1-based -> 0-based copy */
-static int64_t* list_of(const mxArray* a, int64_t* n) {
+/* one side's list (field `name` of out / in): NULL = not given; otherwise a
+ * 1-based -> 0-based copy.  The upper bound N_prop is checked by the library
+ * with the reference's message (cal_smatrix_RGF.m:108-116). */
+static int64_t* list_of(const mxArray* a, const char* kind, const char* name, int64_t* n) {
   *n = 0;
   if (!a) return NULL;
   const mwSize k = mxGetNumberOfElements(a);
@@ -115,7 +121,7 @@ static int64_t* list_of(const mxArray* a, int64_t* n) {
   const double* d = mxGetDoubles(a);
   for (mwSize i = 0; i < k; i++) {
     if (!d || d[i] != (double)(int64_t)d[i] || d[i] < 1)
-      mexErrMsgIdAndTxt("rgf:arg", "channel indices must be positive integers");
+      mexErrMsgIdAndTxt("rgf:arg", "%s.%s, when specified, must be an array of positive integers", kind, name);
     out[i] = (int64_t)d[i] - 1;
   }
   *n = (int64_t)k;
@@ -127,24 +133,31 @@ static void side_req(const mxArray* a, const char* kind, const int64_t** L, int6
                      int64_t* nR) {
   *L = *R = NULL;
   *nL = *nR = 0;
-  if (mxIsCell(a)) {
+  if (mxIsCell(a)) {  /* cal_smatrix_RGF.m:120-135 */
     for (mwSize i = 0; i < mxGetNumberOfElements(a); i++) {
       const mxArray* c = mxGetCell(a, i);
       char buf[16] = {0};
-      if (!c || !mxIsChar(c)) continue;
+      if (!c || !mxIsChar(c)) {
+        mexWarnMsgIdAndTxt("rgf:ignored",
+                           "element %s{%d} has wrong format and is ignored; should be one of {'left', 'right', 'L', 'R'}",
+                           kind, (int)i + 1);
+        continue;
+      }
       mxGetString(c, buf, sizeof(buf));
-      if (!strcmp(buf, "left")) *nL = RGF_ALL;
-      else if (!strcmp(buf, "right")) *nR = RGF_ALL;
-      else mexWarnMsgIdAndTxt("rgf:ignored", "%s{%d} = '%s' is not 'left' or 'right'; ignored", kind, (int)i + 1, buf);
+      if (!strcmp(buf, "left") || !strcmp(buf, "L")) *nL = RGF_ALL;
+      else if (!strcmp(buf, "right") || !strcmp(buf, "R")) *nR = RGF_ALL;
+      else
+        mexWarnMsgIdAndTxt("rgf:ignored", "element %s{%d} = %s ignored; should be one of {'left', 'right', 'L', 'R'}",
+                           kind, (int)i + 1, buf);
     }
     return;
   }
-  if (!mxIsStruct(a)) mexErrMsgIdAndTxt("rgf:arg", "%s must be a cell array or a structure", kind);
+  if (!mxIsStruct(a)) mexErrMsgIdAndTxt("rgf:arg", "input argument '%s' must be a structure or a cell array", kind);
   char fl[16], fr[16];
   snprintf(fl, sizeof(fl), "ind_%s_L", kind);
   snprintf(fr, sizeof(fr), "ind_%s_R", kind);
-  *L = list_of(mxGetField(a, 0, fl), nL);
-  *R = list_of(mxGetField(a, 0, fr), nR);
+  *L = list_of(mxGetField(a, 0, fl), kind, fl, nL);
+  *R = list_of(mxGetField(a, 0, fr), kind, fr, nR);
 }
 
 static mxArray* cplx_vec(const rgf_cplx* v, mwSize n) {
@@ -208,6 +221,12 @@ static mxArray* chbuf_struct(const chbuf* b, int64_t N, int dim) {
   }
   for (int k = 0; k < 2; k++) {
     const int64_t np = k ? b->c.N_prop_R : b->c.N_prop_L;
+    if (k == 1 && np < 0) {  /* one-sided set-up: channels.R.N_prop = NaN (setup_channels.m:171-174) */
+      mxArray* t = mxCreateStructMatrix(1, 1, 1, side);
+      mxSetField(t, 0, "N_prop", mxCreateDoubleScalar(NAN));
+      mxSetField(s, 0, "R", t);
+      continue;
+    }
     mxArray* t = mxCreateStructMatrix(1, 1, b->c.has_prop_conj ? 5 : 4, side);
     mxSetField(t, 0, "N_prop", mxCreateDoubleScalar((double)np));
     mxSetField(t, 0, "kxdx", cplx_vec(k ? b->kxR : b->kxL, N));

@@ -22,6 +22,18 @@ from .rgf_ref import (_delta_matrix, build_laplacian_1d, parse_channel_request,
 
 
 def smatrix_dense_2d(syst, out, in_):
+    """S of cal_smatrix_RGF from a dense solve of the whole operator."""
+    return _dense_2d(syst, out, in_, fields=False)
+
+
+def fields_dense_2d(syst, out, in_):
+    """(S, psi): psi[:, n, b] = G_{n+1, side(b)} B_b, the response at slice n
+    (site n+1) to input channel b (columns in S's order [in_L; in_R]), from
+    the same dense inverse."""
+    return _dense_2d(syst, out, in_, fields=True)
+
+
+def _dense_2d(syst, out, in_, fields):
     eps = np.asarray(syst["epsilon"], dtype=complex)
     ny, nx = eps.shape
     k0dx = syst["k0dx"]
@@ -58,4 +70,12 @@ def smatrix_dense_2d(syst, out, in_):
     C_R = chR["sqrt_mu"][ioR - 1][:, None] * phi[:, chR["ind_prop"][ioR - 1] - 1].conj().T
     S = (-2j) * np.block([[C_L @ G_LL @ B_L, C_L @ G_LR @ B_R],
                           [C_R @ G_RL @ B_L, C_R @ G_RR @ B_R]])
-    return S - _delta_matrix(ioL, ioR, iiL, iiR)
+    S = S - _delta_matrix(ioL, ioR, iiL, iiR)
+    if not fields:
+        return S
+    psi = np.zeros((N, nx, B_L.shape[1] + B_R.shape[1]), dtype=complex)
+    for n in range(nx):
+        r = slice((n + 1) * N, (n + 2) * N)
+        psi[:, n, :B_L.shape[1]] = Ginv[r, 0:N] @ B_L
+        psi[:, n, B_L.shape[1]:] = Ginv[r, (nsite - 1) * N:] @ B_R
+    return S, psi

@@ -17,13 +17,15 @@ import numpy as np
 LIB_PATH = Path(__file__).resolve().parent / "librgf.so"
 
 RGF_OK, RGF_ERR_ARG, RGF_ERR_NONFINITE, RGF_ERR_SINGULAR, RGF_ERR_TIMEOUT, RGF_ERR_CUDA, RGF_ERR_OOM, \
-    RGF_ERR_NODEVICE = range(8)
+    RGF_ERR_NODEVICE, RGF_ERR_ILLCOND = range(9)
 STATUS_NAMES = {0: "RGF_OK", 1: "RGF_ERR_ARG", 2: "RGF_ERR_NONFINITE", 3: "RGF_ERR_SINGULAR",
-                4: "RGF_ERR_TIMEOUT", 5: "RGF_ERR_CUDA", 6: "RGF_ERR_OOM", 7: "RGF_ERR_NODEVICE"}
+                4: "RGF_ERR_TIMEOUT", 5: "RGF_ERR_CUDA", 6: "RGF_ERR_OOM", 7: "RGF_ERR_NODEVICE",
+                8: "RGF_ERR_ILLCOND"}
 
 BC_PERIODIC, BC_DIRICHLET, BC_NEUMANN, BC_DIRICHLET_NEUMANN, BC_NEUMANN_DIRICHLET, BC_BLOCH = range(6)
 RGF_ALL = -1
 RGF_FP64 = 0
+RGF_NOALLOC_SCRATCH_BYTES = 32 << 20  # include/rgf.h
 
 
 class Cplx(ctypes.Structure):
@@ -76,6 +78,18 @@ SIGNATURES = {
                                     c_int64, c_void_p, c_int64, c_void_p, c_int64]),
     "rgf_smatrix_grad_3d": (c_int, [c_void_p, POINTER(Syst3D), POINTER(Request), POINTER(Options), c_void_p,
                                     c_int64, c_void_p, c_int64, c_void_p, c_int64]),
+    "rgf_fields_2d": (c_int, [c_void_p, POINTER(Syst2D), POINTER(Request), POINTER(Options), c_void_p, c_int64,
+                              c_void_p, c_int64]),
+    "rgf_fields_3d": (c_int, [c_void_p, POINTER(Syst3D), POINTER(Request), POINTER(Options), c_void_p, c_int64,
+                              c_void_p, c_int64]),
+    "rgf_segment_sweep_2d": (c_int, [c_void_p, POINTER(Syst2D), POINTER(Request), POINTER(Options), c_int32,
+                                     c_int64, c_void_p]),
+    "rgf_segment_sweep_3d": (c_int, [c_void_p, POINTER(Syst3D), POINTER(Request), POINTER(Options), c_int32,
+                                     c_int64, c_void_p]),
+    "rgf_segment_merge_2d": (c_int, [c_void_p, POINTER(Syst2D), POINTER(Request), POINTER(Options), c_void_p,
+                                     c_void_p, c_void_p, c_int64]),
+    "rgf_segment_merge_3d": (c_int, [c_void_p, POINTER(Syst3D), POINTER(Request), POINTER(Options), c_void_p,
+                                     c_void_p, c_void_p, c_int64]),
     "rgf_smatrix_size_2d": (c_int, [c_void_p, POINTER(Syst2D), POINTER(Request), POINTER(c_int64),
                                     POINTER(c_int64)]),
     "rgf_smatrix_size_3d": (c_int, [c_void_p, POINTER(Syst3D), POINTER(Request), POINTER(c_int64),
@@ -88,6 +102,7 @@ SIGNATURES = {
     "rgf_last_error": (c_char_p, []),
     "rgf_version": (c_char_p, []),
     "rgf_last_stats": (c_int, [c_void_p, POINTER(c_int64), POINTER(c_double)]),
+    "rgf_last_engine": (c_int, [c_void_p, POINTER(c_int32), POINTER(c_int32), POINTER(c_double)]),
     "rgf_last_profile": (c_int, [c_void_p, POINTER(c_int64), POINTER(c_double), POINTER(c_double), c_char_p,
                                  ctypes.c_size_t]),
     "rgf_set_stream": (c_int, [c_void_p, c_void_p]),
@@ -121,7 +136,19 @@ def load() -> ctypes.CDLL:
     return _lib
 
 
+class IllConditionedWarning(UserWarning):
+    """A slice inverse failed its a-posteriori check even under partial
+    pivoting over the whole column (RGF_ERR_ILLCOND): the result is returned
+    but may be inaccurate -- where MATLAB's inv warns that the matrix is close
+    to singular or badly scaled."""
+
+
 def check(status: int) -> None:
+    if status == RGF_ERR_ILLCOND:
+        import warnings
+        msg = load().rgf_last_error()
+        warnings.warn(msg.decode() if msg else "ill-conditioned slice matrix", IllConditionedWarning, stacklevel=3)
+        return
     if status != RGF_OK:
         msg = load().rgf_last_error()
         raise RGFError(status, msg.decode() if msg else "")
@@ -158,6 +185,12 @@ class Handle:
         name = ctypes.create_string_buffer(128)
         check(self.lib.rgf_last_profile(self.h, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(fl), name, 128))
         return int(n.value), float(ms.value), float(fl.value), name.value.decode()
+
+    def engine(self):
+        """(engine, fallback, rejected probe residual) of the last S-matrix call."""
+        e, f, r = c_int32(), c_int32(), c_double()
+        check(self.lib.rgf_last_engine(self.h, ctypes.byref(e), ctypes.byref(f), ctypes.byref(r)))
+        return int(e.value), int(f.value), float(r.value)
 
     def stats(self):
         n = c_int64()

@@ -380,6 +380,61 @@ def smatrix_grad_RGF_3D(syst, out, in_, D, *, checkpoint: int = 0, device: int =
     return S, g
 
 
+def fields_RGF(syst, out, in_, *, checkpoint: int = 0, device: int = 0, options=None, handle=None):
+    """(S, psi) for a 2D syst: S as cal_smatrix_RGF, and the fields inside the
+    structure psi[m, n, b] = (G_{n, s(b)} B_b)_m -- the response at site m of
+    slice n to input channel b (the columns of S) -- of shape [ny, nx, n_in].
+    An addition of this library (the reference points to MESTI for fields)."""
+    _check_syst(syst, "yBC")
+    eps = np.asarray(_get(syst, "epsilon"))
+    if eps.ndim != 2 or not np.issubdtype(eps.dtype, np.number):
+        raise ValueError("syst.epsilon must be a numeric matrix")
+    ny, nx = eps.shape
+    bc, ka = _bc_2d(_get(syst, "yBC"))
+    req, keep = _request(out, in_)
+    h = handle or _abi.default_handle(device)
+    epsf = np.ascontiguousarray(eps.astype(complex).ravel(order="F"))
+    sy = Syst2D(ny, nx, ptr(epsf), 0, cplx(_get(syst, "epsilon_L")), cplx(_get(syst, "epsilon_R")),
+                cplx(_get(syst, "k0dx")), bc, ka)
+    no, ni = ctypes.c_int64(), ctypes.c_int64()
+    check(h.lib.rgf_smatrix_size_2d(h.h, ctypes.byref(sy), ctypes.byref(req), ctypes.byref(no), ctypes.byref(ni)))
+    S = np.zeros((max(no.value, 1), max(ni.value, 1)), dtype=complex, order="F")
+    psi = np.zeros((ny, nx, ni.value), dtype=complex, order="F")
+    pp = psi if psi.size else np.zeros(1, dtype=complex)
+    opt = _options(options)
+    check(h.lib.rgf_fields_2d(h.h, ctypes.byref(sy), ctypes.byref(req), ctypes.byref(opt), S.ctypes.data,
+                              S.shape[0], pp.ctypes.data, int(checkpoint)))
+    del keep
+    S = S[:no.value, :ni.value] if (no.value and ni.value) else np.zeros((no.value, ni.value))
+    return S, psi
+
+
+def fields_RGF_3D(syst, out, in_, *, checkpoint: int = 0, device: int = 0, options=None, handle=None):
+    """(S, psi) for a 3D syst; psi has shape [nx, ny, nz, n_in]."""
+    _check_syst(syst, "xyBC")
+    eps = np.asarray(_get(syst, "epsilon"))
+    if eps.ndim == 2:
+        eps = eps[:, :, None]
+    nx, ny, nz = eps.shape
+    bc, kxa, kya = _bc_3d(_get(syst, "xyBC"))
+    req, keep = _request(out, in_)
+    h = handle or _abi.default_handle(device)
+    epsf = np.ascontiguousarray(eps.astype(complex).ravel(order="F"))
+    sy = Syst3D(nx, ny, nz, ptr(epsf), 0, cplx(_get(syst, "epsilon_L")), cplx(_get(syst, "epsilon_R")),
+                cplx(_get(syst, "k0dx")), bc, kxa, kya)
+    no, ni = ctypes.c_int64(), ctypes.c_int64()
+    check(h.lib.rgf_smatrix_size_3d(h.h, ctypes.byref(sy), ctypes.byref(req), ctypes.byref(no), ctypes.byref(ni)))
+    S = np.zeros((max(no.value, 1), max(ni.value, 1)), dtype=complex, order="F")
+    psi = np.zeros((nx, ny, nz, ni.value), dtype=complex, order="F")
+    pp = psi if psi.size else np.zeros(1, dtype=complex)
+    opt = _options(options)
+    check(h.lib.rgf_fields_3d(h.h, ctypes.byref(sy), ctypes.byref(req), ctypes.byref(opt), S.ctypes.data,
+                              S.shape[0], pp.ctypes.data, int(checkpoint)))
+    del keep
+    S = S[:no.value, :ni.value] if (no.value and ni.value) else np.zeros((no.value, ni.value))
+    return S, psi
+
+
 def _one_sided(epsilon_R) -> bool:
     return epsilon_R is None or (np.isscalar(epsilon_R) and np.isnan(epsilon_R))
 

@@ -16,6 +16,11 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 OUT = PKG / "librgf.so"
 PEAK_OUT = PKG / "librgf_peak.so"
+SELFTEST_SRC = PKG.parent / "tests" / "cuda" / "selftest.cu"
+SELFTEST_OUT = PKG.parent / "tests" / "cuda" / "libselftest.so"
+MEXSTUB_DIR = PKG.parent / "tests" / "mexstub"
+MEXSTUB_OUT = MEXSTUB_DIR / "libmexstub.so"
+MEX_GATEWAY = PKG.parent / "matlab" / "rgf_mex.c"
 SOURCES = ["channels.cu", "sweep.cu", "persist.cu", "rgf_api.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
@@ -36,6 +41,8 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         newest = max(p.stat().st_mtime for p in deps)
         if OUT.stat().st_mtime >= newest:
             build_peak(verbose, force)
+            build_selftest(verbose, force)
+            build_mexstub(verbose, force)
             return OUT
     objdir = PKG / "_build"
     objdir.mkdir(exist_ok=True)
@@ -54,6 +61,8 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     subprocess.run(cmd, check=True)
     os.replace(tmp, OUT)
     build_peak(verbose, force)
+    build_selftest(verbose, force)
+    build_mexstub(verbose, force)
     return OUT
 
 
@@ -68,6 +77,44 @@ def build_peak(verbose: bool = False, force: bool = False) -> Path:
     subprocess.run(cmd, check=True)
     os.replace(tmp, PEAK_OUT)
     return PEAK_OUT
+
+
+def build_selftest(verbose: bool = False, force: bool = False) -> Path:
+    """Unit-test kernels for device functions without a C-ABI entry (tests only)."""
+    if not SELFTEST_SRC.exists():
+        return SELFTEST_OUT
+    deps = [SELFTEST_SRC, CSRC / "recip.cuh", CSRC / "rgf_internal.cuh"]
+    if SELFTEST_OUT.exists() and not force and SELFTEST_OUT.stat().st_mtime >= max(p.stat().st_mtime for p in deps):
+        return SELFTEST_OUT
+    tmp = SELFTEST_OUT.with_suffix(".so.tmp")
+    cmd = [nvcc(), *ARCH, *FLAGS, "-I", str(PKG.parent / "include"), "-shared", "-cudart", "static", "-o", str(tmp),
+           str(SELFTEST_SRC)]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, SELFTEST_OUT)
+    return SELFTEST_OUT
+
+
+def build_mexstub(verbose: bool = False, force: bool = False) -> Path:
+    """The MEX gateway (matlab/rgf_mex.c) compiled against the test harness's
+    stand-in for MATLAB's MEX API (tests/mexstub), linked to librgf.so: lets
+    the tests drive mexFunction without MATLAB."""
+    src = MEXSTUB_DIR / "mexstub.c"
+    if not src.exists():
+        return MEXSTUB_OUT
+    deps = [src, MEXSTUB_DIR / "mex.h", MEX_GATEWAY, PKG.parent / "include" / "rgf.h", OUT]
+    if MEXSTUB_OUT.exists() and not force and MEXSTUB_OUT.stat().st_mtime >= max(p.stat().st_mtime for p in deps):
+        return MEXSTUB_OUT
+    tmp = MEXSTUB_OUT.with_suffix(".so.tmp")
+    cmd = [os.environ.get("CC", "gcc"), "-std=gnu11", "-O2", "-Wall", "-shared", "-fPIC", "-fvisibility=hidden",
+           "-I", str(MEXSTUB_DIR), "-I", str(PKG.parent / "include"), str(src), str(MEX_GATEWAY),
+           "-L", str(PKG), "-lrgf", "-Wl,-rpath,$ORIGIN/../../rgf_b200", "-o", str(tmp)]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, MEXSTUB_OUT)
+    return MEXSTUB_OUT
 
 
 if __name__ == "__main__":

@@ -47,6 +47,7 @@
 #include <math.h>
 
 #include "persist.cuh"
+#include "recip.cuh"
 
 namespace rgf {
 
@@ -115,23 +116,6 @@ __device__ __forceinline__ unsigned long long gtimer() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
   return t;
-}
-
-// 1/z = conj(z) r with r = 1/|z|^2 by the Newton-Raphson iteration for a
-// reciprocal, r <- r + r (1 - n r) (quadratic convergence), started from
-// rcp.approx.ftz.f64 and run twice: the result is within a few ulp of the
-// correctly rounded 1/n for every |z|^2 in the normal double range.
-// Branch-free, so every lane of a warp can form it speculatively; |z|^2 = 0
-// or subnormal gives a non-finite result, which the caller flags as singular.
-__device__ __forceinline__ double2 crecip_nr(double2 z) {
-  const double n = fma(z.x, z.x, z.y * z.y);
-  double r;
-  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(n));
-  double e = fma(-n, r, 1.0);
-  r = fma(r, e, r);
-  e = fma(-n, r, 1.0);
-  r = fma(r, e, r);
-  return cmk(z.x * r, -z.y * r);
 }
 
 // swizzled element positions of the staged operand tiles (conflict-free
@@ -309,7 +293,8 @@ __device__ double boundary_pass(const PersistParams& p, int I, int Cq, int tid, 
       if (i < p.N) {
         const double2 v = probe_v(i);
         const double2 d = csub(__ldcg(w2), v);
-        pmax = fmax(pmax, sqrt(cabs2(d)));
+        const double rr = sqrt(cabs2(d));
+        pmax = (rr == rr) ? fmax(pmax, rr) : INFINITY;  // fmax would drop a NaN
         if (eps_next) {
           double2 Av = cmk(0.0, 0.0);
           for (int q = 0; q < kMaxStencil; q++) {
@@ -957,7 +942,9 @@ __device__ __forceinline__ bool gj_ahead(const PersistParams& p, Shared& sh, dou
         }
         if (lane == 0) sh.perm[q] = pv;
         st_release_cta(&sh.gflag[lane], q + 1);
-        sing = sing || (best >> 6) == 0u || !isfinite(d.x) || !isfinite(d.y);
+        // a zero reciprocal of a nonzero pivot (|z|^2 beyond the range of
+        // rcp.approx.ftz) is as unusable as a non-finite one
+        sing = sing || (best >> 6) == 0u || !isfinite(d.x) || !isfinite(d.y) || (d.x == 0.0 && d.y == 0.0);
         used |= 1u << pv;
 #pragma unroll
         for (int c = 0; c < NC; c++) {

@@ -41,7 +41,6 @@ struct Arena {
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
-  Arena* arena = nullptr;  // non-null: grow inside this arena instead of cudaMalloc
 };
 
 }  // namespace rgf
@@ -59,8 +58,10 @@ struct rgf_handle_s {
   // workspace (grow-only)
   DevBuf k0, k1, kx[2], lam[2], mu[2], isprop[2], prop[2], conj[2], nprop, status;
   DevBuf phi, tmp, g0s, g0e, st_col, st_val, eps, aug, pc, u, idx, sdev;
-  DevBuf xpc, xrow, xt, xu, xsync, xprobe, xtrace;  // persistent-kernel exchange buffers
+  DevBuf xpc, xrow, xt, xu, xsync, xprobe;  // persistent-kernel exchange buffers
   DevBuf gck, gseg, gm0, gpsi, gphi, get, gd, gg;   // permittivity gradient (checkpoints, carriers)
+  DevBuf gf;                                        // fields staged for a host output
+  DevBuf segs;                                      // segment states staged for a merge
   int sms = 0;
   // batched calls: one sub-handle per concurrent pipeline (own stream and
   // workspace, a share of the SMs for its persistent sweeps)
@@ -70,6 +71,13 @@ struct rgf_handle_s {
   int64_t launches = 0;
   std::string prof_kernel;
   double probe = 0.0;
+  DevBuf gepp;  // scratch of the whole-column pivoting (per-step engine)
+  int engine_used = 0;     // engine of the last call's final run
+  int fallback = 0;        // 1: the persistent engine's result was rejected and recomputed
+  double probe_first = 0;  // probe residual of the rejected run
+  // non-null: every workspace buffer is carved from this arena and nothing is
+  // ever allocated (the handle of rgf_smatrix_2d_noalloc)
+  Arena* arena = nullptr;
 };
 
 namespace {
@@ -83,19 +91,20 @@ namespace {
     }                                                                              \
   } while (0)
 
-rgf_status ensure(DevBuf& b, size_t bytes) {
+rgf_status ensure(rgf_handle h, DevBuf& b, size_t bytes) {
   if (bytes == 0) bytes = 16;
   if (b.bytes >= bytes) return RGF_OK;
-  if (b.arena) {
+  if (h->arena) {  // never cudaMalloc on an allocation-free handle
+    Arena* a = h->arena;
     const size_t need = (bytes + 255) & ~(size_t)255;
-    if (b.arena->used + need > b.arena->cap) {
+    if (a->used + need > a->cap) {
       set_error("problem too large for the static device scratch of rgf_smatrix_2d_noalloc (" +
-                std::to_string(b.arena->cap >> 20) + " MiB): its workspace needs more; use rgf_smatrix_2d");
+                std::to_string(a->cap >> 20) + " MiB): its workspace needs more; use rgf_smatrix_2d");
       return RGF_ERR_ARG;
     }
-    b.p = b.arena->base + b.arena->used;
+    b.p = a->base + a->used;
     b.bytes = bytes;
-    b.arena->used += need;
+    a->used += need;
     return RGF_OK;
   }
   if (b.p) cudaFree(b.p);
@@ -156,17 +165,17 @@ rgf_status run_channels(rgf_handle h, const Transverse& tr, double2 k2eL, double
                         ChanInfo* ci) {
   const int64_t N = tr.N;
   rgf_status st;
-  if ((st = ensure(h->k0, sizeof(double) * tr.n0))) return st;
-  if ((st = ensure(h->k1, sizeof(double) * tr.n1))) return st;
+  if ((st = ensure(h, h->k0, sizeof(double) * tr.n0))) return st;
+  if ((st = ensure(h, h->k1, sizeof(double) * tr.n1))) return st;
   for (int s = 0; s < 2; s++) {
-    if ((st = ensure(h->kx[s], sizeof(double2) * N))) return st;
-    if ((st = ensure(h->lam[s], sizeof(double2) * N))) return st;
-    if ((st = ensure(h->mu[s], sizeof(double2) * N))) return st;
-    if ((st = ensure(h->isprop[s], sizeof(int) * N))) return st;
-    if ((st = ensure(h->prop[s], sizeof(int) * N))) return st;
-    if ((st = ensure(h->conj[s], sizeof(int) * N))) return st;
+    if ((st = ensure(h, h->kx[s], sizeof(double2) * N))) return st;
+    if ((st = ensure(h, h->lam[s], sizeof(double2) * N))) return st;
+    if ((st = ensure(h, h->mu[s], sizeof(double2) * N))) return st;
+    if ((st = ensure(h, h->isprop[s], sizeof(int) * N))) return st;
+    if ((st = ensure(h, h->prop[s], sizeof(int) * N))) return st;
+    if ((st = ensure(h, h->conj[s], sizeof(int) * N))) return st;
   }
-  if ((st = ensure(h->nprop, sizeof(int) * 2))) return st;
+  if ((st = ensure(h, h->nprop, sizeof(int) * 2))) return st;
   ci->two_sided = two_sided;
   ci->same = !two_sided || (k2eL.x == k2eR.x && k2eL.y == k2eR.y);
   int conj_mode = 0;
@@ -243,7 +252,8 @@ rgf_status copy_channels_out(rgf_handle h, const Transverse& tr, const ChanInfo&
 }
 
 // resolve one side's channel list (cal_smatrix_RGF.m:103-178)
-rgf_status resolve_list(const int64_t* ind, int64_t n, int64_t np, const char* name, std::vector<int>* out) {
+rgf_status resolve_list(const int64_t* ind, int64_t n, int64_t np, const char* name, char side,
+                        std::vector<int>* out) {
   out->clear();
   if (n == RGF_ALL) {
     for (int64_t p = 0; p < np; p++) out->push_back((int)p);
@@ -259,8 +269,8 @@ rgf_status resolve_list(const int64_t* ind, int64_t n, int64_t np, const char* n
   }
   for (int64_t k = 0; k < n; k++) {
     if (ind[k] < 0 || ind[k] >= np) {
-      set_error(std::string(name) + ", when specified, must be an array of positive integers not exceeding N_prop=" +
-                std::to_string(np));
+      set_error(std::string(name) + ", when specified, must be an array of positive integers not exceeding N_prop_" +
+                side + "=" + std::to_string(np));
       return RGF_ERR_ARG;
     }
     out->push_back((int)ind[k]);
@@ -289,10 +299,10 @@ struct Request {
 
 rgf_status resolve_request(const rgf_request* req, const ChanInfo& ci, Request* r) {
   rgf_status st;
-  if ((st = resolve_list(req->ind_out_L, req->n_out_L, ci.np[0], "out.ind_out_L", &r->out[0]))) return st;
-  if ((st = resolve_list(req->ind_out_R, req->n_out_R, ci.np[1], "out.ind_out_R", &r->out[1]))) return st;
-  if ((st = resolve_list(req->ind_in_L, req->n_in_L, ci.np[0], "in.ind_in_L", &r->in[0]))) return st;
-  if ((st = resolve_list(req->ind_in_R, req->n_in_R, ci.np[1], "in.ind_in_R", &r->in[1]))) return st;
+  if ((st = resolve_list(req->ind_out_L, req->n_out_L, ci.np[0], "out.ind_out_L", 'L', &r->out[0]))) return st;
+  if ((st = resolve_list(req->ind_out_R, req->n_out_R, ci.np[1], "out.ind_out_R", 'R', &r->out[1]))) return st;
+  if ((st = resolve_list(req->ind_in_L, req->n_in_L, ci.np[0], "in.ind_in_L", 'L', &r->in[0]))) return st;
+  if ((st = resolve_list(req->ind_in_R, req->n_in_R, ci.np[1], "in.ind_in_R", 'R', &r->in[1]))) return st;
   return RGF_OK;
 }
 
@@ -371,18 +381,48 @@ rgf_status smatrix_sizes(rgf_handle h, const Problem& p, const rgf_request* req,
 // Permittivity gradient request of smatrix(): g[m + n*N] = sum_ab D_ab dS_ab / d eps[m, n]
 // for the weights D (n_out x n_in, column-major, leading dimension ldD, in the
 // row/column order of S); D and g are device pointers when S is.
+//
+// The same backward pass also yields the fields inside the structure: with
+// `psi`, psi[m + n*N + b*N*L] = (G_{n, ends} B)_{m b}, the response at site m
+// of slice n to input channel b (the columns of S), written as each Psi_j
+// is formed.  D == nullptr: fields only (no gradient).
 struct GradReq {
   const rgf_cplx* D;
   int64_t ldD;
   rgf_cplx* g;
   int64_t checkpoint;  // slices per recomputed segment (<= 0: ceil(sqrt(L)))
+  rgf_cplx* psi = nullptr;
 };
 
-rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const rgf_options* opt, rgf_cplx* S,
-                   int64_t ldS, rgf_channels* ch, const GradReq* gr = nullptr) {
+// Largest per-slice probe residual max|G_n M_n v - v| (|v_i| = 1) accepted
+// from the persistent engine, whose pivot search stays inside each 32 x 32
+// pivot block: above it (or on a zero / non-finite pivot) the S-matrix is
+// recomputed by the per-step engine with partial pivoting over the whole
+// column.  Above kProbeIllcond even that result is reported as
+// RGF_ERR_ILLCOND (MATLAB's inv would warn "close to singular").
+constexpr double kProbeRetry = 1e-10;
+constexpr double kProbeIllcond = 1e-8;
+// internal status of smatrix_run: recompute with engine 1
+constexpr rgf_status kRetryWholeColumn = static_cast<rgf_status>(1000);
+
+// Segment sweep of an L-split S-matrix: the slices [0, cut) swept from the
+// left lead (side 0) or [cut, L) from the right lead (side 1), carrying only
+// that side's requested channels, with no far lead; `state` receives W after
+// the segment's last slice, [[g, X], [Z, Y]] row-major with leading dimension
+// N + n_in(side) (g the lead-connected Green's function of the segment's last
+// slice, X = g..g0 B, Z = C g0..g, Y = C G B at the lead).
+struct SegReq {
+  int side;
+  int64_t cut;
+  rgf_cplx* state;
+};
+
+rgf_status smatrix_run(rgf_handle h, const Problem& p, const rgf_request* req, const rgf_options* opt, rgf_cplx* S,
+                       int64_t ldS, rgf_channels* ch, const GradReq* gr, int engine, const SegReq* seg) {
   rgf_status st;
   h->launches = 0;
   h->probe = 0.0;
+  h->engine_used = engine;
   if ((st = validate_problem(p, req))) return st;
   if (opt && opt->precision != RGF_FP64) {
     set_error("unsupported precision form");
@@ -404,34 +444,47 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
   const int noL = (int)rq.out[0].size(), noR = (int)rq.out[1].size();
   const int niL = (int)rq.in[0].size(), niR = (int)rq.in[1].size();
   const int n_out = noL + noR, n_in = niL + niR;
+  if (gr && gr->psi && n_in > 0 && n_out == 0) {
+    set_error("the fields are computed with S: request at least one output channel");
+    return RGF_ERR_ARG;
+  }
   if (n_out == 0 || n_in == 0) {  // :181-184
-    if (gr && L > 0) {  // S is empty: so is its derivative
+    if (gr && gr->D && L > 0) {  // S is empty: so is its derivative
       if (S_dev) RGF_CUDA_TRY(cudaMemsetAsync(gr->g, 0, sizeof(rgf_cplx) * N * L, h->stream));
       else memset(gr->g, 0, sizeof(rgf_cplx) * N * L);
     }
     return copy_channels_out(h, tr, ci, ch);
   }
-  if (gr && gr->ldD < n_out) {
+  if (gr && gr->D && gr->ldD < n_out) {
     set_error("ldD must be >= the number of requested output channels");
     return RGF_ERR_ARG;
   }
-  if (!S) {
+  if (seg && (seg->cut <= 0 || seg->cut >= L || !seg->state || (seg->side != 0 && seg->side != 1))) {
+    set_error("segment: need 0 < cut < L (each part at least one slice), side 0 or 1 and a state buffer");
+    return RGF_ERR_ARG;
+  }
+  if (!S && !seg) {
     set_error("S must not be NULL");
     return RGF_ERR_ARG;
   }
-  if (ldS < n_out) {
+  if (!seg && ldS < n_out) {
     set_error("ldS must be >= the number of requested output channels");
     return RGF_ERR_ARG;
   }
 
   // (2) recursion direction: right-to-left when nothing enters from the
   // right (cal_smatrix_RGF.m:217-236), left-to-right otherwise (:237-280)
-  const bool mirror = (niR == 0);
+  // (a segment sweep goes from its own lead and carries that side only)
+  const bool mirror = seg ? seg->side == 1 : (niR == 0);
   const int s = mirror ? 1 : 0, e = 1 - s;
+  static const std::vector<int> kNone;
   const std::vector<int>& in_s = rq.in[s];
   const std::vector<int>& out_s = rq.out[s];
-  const std::vector<int>& in_e = rq.in[e];
-  const std::vector<int>& out_e = rq.out[e];
+  const std::vector<int>& in_e = seg ? kNone : rq.in[e];
+  const std::vector<int>& out_e = seg ? kNone : rq.out[e];
+  // slices swept (in recursion order 0 .. Ls-1; slice k is physical slice
+  // mirror ? L-1-k : k)
+  const int64_t Ls = seg ? (seg->side == 0 ? seg->cut : L - seg->cut) : L;
   const int ni_s = (int)in_s.size(), no_s = (int)out_s.size(), ni_e = (int)in_e.size(), no_e = (int)out_e.size();
   const int64_t R = N + no_s + no_e, C = N + ni_s + ni_e;
   // persistent engine: active R_p x C_p with the probe pair at an even column
@@ -440,17 +493,17 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
   const int kSwW = sweep_block_width();
 
   // (3) workspace
-  if ((st = ensure(h->phi, sizeof(double2) * N * N))) return st;
-  if ((st = ensure(h->tmp, sizeof(double2) * N * N))) return st;
-  if ((st = ensure(h->g0s, sizeof(double2) * N * N))) return st;
-  if (!ci.same && (st = ensure(h->g0e, sizeof(double2) * N * N))) return st;
-  if ((st = ensure(h->st_col, sizeof(int) * N * kMaxStencil))) return st;
-  if ((st = ensure(h->st_val, sizeof(double2) * N * kMaxStencil))) return st;
-  if ((st = ensure(h->aug, sizeof(double2) * R * ldm))) return st;
-  if ((st = ensure(h->pc, sizeof(double2) * std::max(R, Cp) * kSwW))) return st;
-  if ((st = ensure(h->u, sizeof(double2) * kSwW * ldm))) return st;
-  if ((st = ensure(h->status, sizeof(int)))) return st;
-  if (!S_dev && (st = ensure(h->sdev, sizeof(double2) * (int64_t)n_out * n_in))) return st;
+  if ((st = ensure(h, h->phi, sizeof(double2) * N * N))) return st;
+  if ((st = ensure(h, h->tmp, sizeof(double2) * N * N))) return st;
+  if ((st = ensure(h, h->g0s, sizeof(double2) * N * N))) return st;
+  if (!ci.same && (st = ensure(h, h->g0e, sizeof(double2) * N * N))) return st;
+  if ((st = ensure(h, h->st_col, sizeof(int) * N * kMaxStencil))) return st;
+  if ((st = ensure(h, h->st_val, sizeof(double2) * N * kMaxStencil))) return st;
+  if ((st = ensure(h, h->aug, sizeof(double2) * R * ldm))) return st;
+  if ((st = ensure(h, h->pc, sizeof(double2) * std::max(R, Cp) * kSwW))) return st;
+  if ((st = ensure(h, h->u, sizeof(double2) * kSwW * ldm))) return st;
+  if ((st = ensure(h, h->status, sizeof(int)))) return st;
+  if (!S_dev && (st = ensure(h, h->sdev, sizeof(double2) * (int64_t)n_out * n_in))) return st;
   // index arrays: in_s, out_s, in_e, out_e, row_of, col_of, delta pairs
   std::vector<int> row_of(n_out), col_of(n_in), pairs;
   for (int o = 0; o < n_out; o++) {
@@ -477,7 +530,7 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
   };
   size_t o_in_s = push(in_s), o_out_s = push(out_s), o_in_e = push(in_e), o_out_e = push(out_e);
   size_t o_row = push(row_of), o_col = push(col_of), o_pairs = push(pairs);
-  if ((st = ensure(h->idx, sizeof(int) * (idx.size() + 1)))) return st;
+  if ((st = ensure(h, h->idx, sizeof(int) * (idx.size() + 1)))) return st;
   int* idx_d = as<int>(h->idx);
   RGF_CUDA_TRY(cudaMemcpyAsync(idx_d, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, h->stream));
   int* status = as<int>(h->status);
@@ -489,7 +542,7 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
     if (p.eps_dev) {
       eps_d = reinterpret_cast<const double2*>(p.eps);
     } else {
-      if ((st = ensure(h->eps, sizeof(double2) * N * L))) return st;
+      if ((st = ensure(h, h->eps, sizeof(double2) * N * L))) return st;
       RGF_CUDA_TRY(cudaMemcpyAsync(h->eps.p, p.eps, sizeof(double2) * N * L, cudaMemcpyHostToDevice, h->stream));
       eps_d = as<double2>(h->eps);
     }
@@ -539,7 +592,7 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
                        idx_d + o_out_e, no_e, h->stream);
     h->launches += 2;
   };
-  if (L > 0) {
+  if (Ls > 0) {
     launch_assemble(M, ldm, N, N, g0s, N, nullptr, 0, st_col, st_val, k2, slice_eps(0), cmk(0, 0), h->stream);
     h->launches++;
   } else {
@@ -550,9 +603,16 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
   const int prof_every = (opt && opt->profile > 0) ? opt->profile : 0;
   size_t ev_used = 0;
   double prof_flops = 0.0;
-  auto sweep = [&](int64_t Ract, int64_t Cact, bool timed) {
+  // One sweep (per-step engine) of the active Ract x Cact matrix.  Per pivot
+  // block: the rows of the whole remaining column are pivoted into place
+  // (partial pivoting as in LAPACK zgetrf), the block is inverted and the
+  // rank-32 update applied; at the end the column exchanges are undone.
+  if ((st = ensure(h, h->gepp, gepp_scratch_bytes(N)))) return st;
+  auto sweep = [&](int64_t Ract, int64_t Cact, bool timed) -> rgf_status {
     for (int64_t j0 = 0; j0 < N; j0 += kSwW) {
       int jn = (int)std::min<int64_t>(kSwW, N - j0);
+      launch_gepp_step(M, ldm, N, Cact, j0, jn, h->gepp.p, status, h->stream);
+      h->launches += 2;
       launch_sweep_panel(M, ldm, Ract, Cact, j0, jn, as<double2>(h->pc), as<double2>(h->u), ldm, status,
                          h->stream);
       if (timed) {
@@ -571,15 +631,19 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
       }
       h->launches += 2;
     }
+    RGF_CUDA_TRY(launch_gepp_unpermute(M, ldm, Ract, N, h->gepp.p, h->stream));
+    h->launches += 2;
     return RGF_OK;
   };
   int BMp = 0, BNp = 0;
-  bool use_persist = L > 0 && !(opt && opt->engine == 1) &&
-                     persist_choose_tile(Rp, Cp, h->sms, &BMp, &BNp, h->sm_budget != nullptr);
+  bool use_persist =
+      L > 0 && engine == 0 && persist_choose_tile(Rp, Cp, h->sms, &BMp, &BNp, h->sm_budget != nullptr);
+  bool ran_persist = false;
+  // per-slice probe residual (both engines)
   unsigned long long* probe_d = nullptr;
   h->prof_kernel = sweep_update_kernel_name();
-  if (use_persist) {
-    if ((st = ensure(h->xprobe, sizeof(unsigned long long)))) return st;
+  if (L > 0) {
+    if ((st = ensure(h, h->xprobe, sizeof(unsigned long long)))) return st;
     probe_d = as<unsigned long long>(h->xprobe);
     RGF_CUDA_TRY(cudaMemsetAsync(probe_d, 0, sizeof(unsigned long long), h->stream));
   }
@@ -593,11 +657,11 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
     if (use_persist) {
       const int TR = (int)((Rp + BMp - 1) / BMp), TC = (int)((Cp + BNp - 1) / BNp);
       const int nflags = persist_flag_words(TR, TC), ncons = persist_cons_words(TR, TC);
-      if ((st = ensure(h->xpc, sizeof(double2) * 2 * TR * BMp * 32))) return st;
-      if ((st = ensure(h->xrow, sizeof(double2) * 4 * TC * 32 * BNp))) return st;  // rowbuf, prebuf
-      if ((st = ensure(h->xt, sizeof(double2) * 11 * 32 * 32))) return st;  // tbuf[2], djjbuf, srvbuf[2][2], ybuf[2][2]
-      if ((st = ensure(h->xu, sizeof(double2) * 2 * TC * 32 * BNp))) return st;
-      if ((st = ensure(h->xsync, sizeof(int) * (nflags + ncons + 4)))) return st;
+      if ((st = ensure(h, h->xpc, sizeof(double2) * 2 * TR * BMp * 32))) return st;
+      if ((st = ensure(h, h->xrow, sizeof(double2) * 4 * TC * 32 * BNp))) return st;  // rowbuf, prebuf
+      if ((st = ensure(h, h->xt, sizeof(double2) * 11 * 32 * 32))) return st;  // tbuf[2], djjbuf, srvbuf[2][2], ybuf[2][2]
+      if ((st = ensure(h, h->xu, sizeof(double2) * 2 * TC * 32 * BNp))) return st;
+      if ((st = ensure(h, h->xsync, sizeof(int) * (nflags + ncons + 4)))) return st;
       int* flags = as<int>(h->xsync);
       RGF_CUDA_TRY(cudaMemsetAsync(flags, 0xFF, sizeof(int) * nflags, h->stream));
       RGF_CUDA_TRY(cudaMemsetAsync(flags + nflags, 0, sizeof(int) * (ncons + 4), h->stream));
@@ -646,24 +710,8 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
       // releases its T flag, so every dependent wait runs out
       const char* wh_env = getenv("RGF_TEST_WITHHOLD_T");
       pp.withhold_t = (wh_env && atoi(wh_env) == 1) ? 1 : 0;
-      // RGF_TRACE=<file>: record per-step role timestamps of the first
-      // RGF_TRACE_STEPS (default 128) steps of the first launch.
-      // RGF_WATCH=<seconds> (with RGF_TRACE): if that launch is still running
-      // after that long, the trace recorded so far is read through a second
-      // stream and written, and the call fails with RGF_ERR_TIMEOUT.
-      const char* trace_path = k_lo == 0 ? getenv("RGF_TRACE") : nullptr;
-      const char* watch_env = getenv("RGF_WATCH");
-      const char* steps_env = getenv("RGF_TRACE_STEPS");
-      pp.trace = nullptr;
+      pp.trace = nullptr;  // per-step event timestamps: a development aid, off in the library
       pp.trace_steps = 0;
-      if (trace_path && *trace_path) {
-        pp.trace_steps = steps_env ? std::max(1, std::min(atoi(steps_env), (int)(nsl * pp.NB))) : 128;
-        if ((st = ensure(h->xtrace,
-                         sizeof(unsigned long long) * (size_t)(TR * TC + kPersistExtraCtas) * pp.trace_steps * kTraceEvents)))
-          return st;
-        pp.trace = as<unsigned long long>(h->xtrace);
-        RGF_CUDA_TRY(cudaMemsetAsync(pp.trace, 0, h->xtrace.bytes, h->stream));
-      }
       const bool timed = prof_every > 0;
       if (timed) {
         while (h->ev.size() < ev_used + 2) {
@@ -695,6 +743,7 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
         probe_d = nullptr;
       } else {
         h->launches++;
+        ran_persist = true;
         if (timed) {
           RGF_CUDA_TRY(cudaEventRecord(h->ev[ev_used + 1], h->stream));
           ev_used += 2;
@@ -705,62 +754,24 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
         char nm[64];
         snprintf(nm, sizeof(nm), "k_persist<%d,%d> (FP64 DMMA sweep, all slices)", BMp, BNp);
         h->prof_kernel = nm;
-        bool hung = false;
-        if (pp.trace && watch_env && atof(watch_env) > 0) {
-          const auto t_start = std::chrono::steady_clock::now();
-          for (;;) {
-            const cudaError_t q = cudaStreamQuery(h->stream);
-            if (q == cudaSuccess) break;
-            if (q != cudaErrorNotReady) RGF_CUDA_TRY(q);
-            const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
-            if (el > atof(watch_env)) {
-              hung = true;
-              break;
-            }
-            std::this_thread::sleep_for(std::chrono::milliseconds(10));
-          }
-        }
-        if (pp.trace) {
-          std::vector<unsigned long long> tr((size_t)(TR * TC + kPersistExtraCtas) * pp.trace_steps * kTraceEvents);
-          cudaStream_t rd = h->stream;
-          if (hung) RGF_CUDA_TRY(cudaStreamCreateWithFlags(&rd, cudaStreamNonBlocking));
-          RGF_CUDA_TRY(cudaMemcpyAsync(tr.data(), pp.trace, sizeof(unsigned long long) * tr.size(),
-                                       cudaMemcpyDeviceToHost, rd));
-          std::vector<int> words(nflags + ncons + 1);
-          if (hung)
-            RGF_CUDA_TRY(
-                cudaMemcpyAsync(words.data(), flags, sizeof(int) * words.size(), cudaMemcpyDeviceToHost, rd));
-          RGF_CUDA_TRY(cudaStreamSynchronize(rd));
-          if (hung) {
-            const std::string wpath = std::string(trace_path) + ".flags";
-            if (FILE* fw = fopen(wpath.c_str(), "wb")) {
-              fwrite(words.data(), sizeof(int), words.size(), fw);
-              fclose(fw);
-            }
-          }
-          if (FILE* f = fopen(trace_path, "wb")) {
-            int hdr[4] = {TR, TC, pp.trace_steps, (int)kTraceEvents};
-            fwrite(hdr, sizeof(int), 4, f);
-            fwrite(tr.data(), sizeof(unsigned long long), tr.size(), f);
-            fclose(f);
-          }
-          if (hung) {
-            set_error("persistent sweep still running after RGF_WATCH seconds; trace written");
-            return RGF_ERR_TIMEOUT;
-          }
-        }
         return RGF_OK;
       }
     }
+    // per-step engine: the probe pair rides along as in the persistent one
+    launch_probe_init(M, ldm, N, Rp, pc1, h->stream);
+    h->launches++;
     for (int64_t k = k_lo; k < k_hi; k++) {
-      if ((st = sweep(N + no_s, N + ni_s, prof_every && (k % prof_every) == 0))) return st;
+      if ((st = sweep(N + no_s, Cp, prof_every && (k % prof_every) == 0))) return st;
+      launch_probe_check(M, ldm, N, pc1, probe_d, h->stream);
+      h->launches++;
       if (snap && (k - k_lo) % snap_mod == snap_mod - 1)
         RGF_CUDA_TRY(cudaMemcpyAsync(snap + ((k - k_lo) / snap_mod) * Rp * ldm, M, sizeof(double2) * Rp * ldm,
                                      cudaMemcpyDeviceToDevice, h->stream));
       if (k + 1 < k_hi) {
         launch_assemble(M, ldm, N, N + no_s, M, ldm, nullptr, 0, st_col, st_val, k2, slice_eps(k + 1), cmk(0, 0),
                         h->stream);
-        h->launches++;
+        launch_probe_init(M, ldm, N, Rp, pc1, h->stream);
+        h->launches += 2;
       }
       if (((k + 1) & 63) == 0 && (st = check_launch())) return st;
     }
@@ -777,26 +788,34 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
               ? 1
               : std::max<int64_t>(1, (int64_t)ceil(sqrt((double)L)));
   if (gr && L > 0) {
-    if ((st = ensure(h->gck, sizeof(double2) * Rp * ldm * std::max<int64_t>(1, L / gK)))) return st;
-    if ((st = ensure(h->gm0, sizeof(double2) * Rp * ldm))) return st;
+    if ((st = ensure(h, h->gck, sizeof(double2) * Rp * ldm * std::max<int64_t>(1, L / gK)))) return st;
+    if ((st = ensure(h, h->gm0, sizeof(double2) * Rp * ldm))) return st;
     RGF_CUDA_TRY(cudaMemcpyAsync(h->gm0.p, M, sizeof(double2) * Rp * ldm, cudaMemcpyDeviceToDevice, h->stream));
   }
-  if (L > 0) {
-    if ((st = run_slices(0, L, gr ? as<double2>(h->gck) : nullptr, (int)gK))) return st;
-    attach(false);
+  if (Ls > 0) {
+    if ((st = run_slices(0, Ls, gr ? as<double2>(h->gck) : nullptr, (int)gK))) return st;
+    if (!seg) attach(false);
   }
-  if ((st = sweep(R, C, false))) return st;
+  if (seg) {
+    // the segment's state: W after its last slice (probe columns excluded)
+    const int64_t Cs = N + ni_s;
+    RGF_CUDA_TRY(cudaMemcpy2DAsync(seg->state, sizeof(rgf_cplx) * Cs, M, sizeof(double2) * ldm,
+                                   sizeof(double2) * Cs, Rp, S_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                   h->stream));
+  } else {
+    if ((st = sweep(R, C, false))) return st;
 
-  // (8) Fisher-Lee (cal_smatrix_RGF.m:279-289)
-  double2* Sd = S_dev ? reinterpret_cast<double2*>(S) : as<double2>(h->sdev);
-  const int64_t ldSd = S_dev ? ldS : n_out;
-  launch_extract(M, ldm, N, idx_d + o_row, n_out, idx_d + o_col, n_in, Sd, ldSd, idx_d + o_pairs, npairs,
-                 h->stream);
-  h->launches += 1 + (npairs > 0 ? 1 : 0);
-  if ((st = check_launch())) return st;
-  if (!S_dev) {
-    RGF_CUDA_TRY(cudaMemcpy2DAsync(S, sizeof(rgf_cplx) * ldS, Sd, sizeof(double2) * n_out,
-                                   sizeof(double2) * n_out, n_in, cudaMemcpyDeviceToHost, h->stream));
+    // (8) Fisher-Lee (cal_smatrix_RGF.m:279-289)
+    double2* Sd = S_dev ? reinterpret_cast<double2*>(S) : as<double2>(h->sdev);
+    const int64_t ldSd = S_dev ? ldS : n_out;
+    launch_extract(M, ldm, N, idx_d + o_row, n_out, idx_d + o_col, n_in, Sd, ldSd, idx_d + o_pairs, npairs,
+                   h->stream);
+    h->launches += 1 + (npairs > 0 ? 1 : 0);
+    if ((st = check_launch())) return st;
+    if (!S_dev) {
+      RGF_CUDA_TRY(cudaMemcpy2DAsync(S, sizeof(rgf_cplx) * ldS, Sd, sizeof(double2) * n_out,
+                                     sizeof(double2) * n_out, n_in, cudaMemcpyDeviceToHost, h->stream));
+    }
   }
   // (9) permittivity gradient: the backward recursions
   //     Psi_j = [X_j, 0] + g_j Psi_{j+1},  Phi_j = [Z_j; 0] + Phi_{j+1} g_j
@@ -806,8 +825,11 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
   //     recomputed from its checkpoint with a snapshot after every slice.
   if (gr && L > 0) {
     const int64_t nI = n_in, nO = n_out;
+    const bool want_g = gr->D != nullptr, want_f = gr->psi != nullptr;
     std::vector<rgf_cplx> Du((size_t)nO * nI), Da((size_t)nO * nI);
-    if (S_dev) {
+    if (!want_g) {
+      // fields only: no weights
+    } else if (S_dev) {
       RGF_CUDA_TRY(cudaMemcpy2DAsync(Du.data(), sizeof(rgf_cplx) * nO, gr->D, sizeof(rgf_cplx) * gr->ldD,
                                      sizeof(rgf_cplx) * nO, nI, cudaMemcpyDeviceToHost, h->stream));
       RGF_CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -817,19 +839,22 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
     }
     for (int64_t i = 0; i < nI; i++)
       for (int64_t o = 0; o < nO; o++) Da[(size_t)row_of[o] * nI + col_of[i]] = Du[o + i * nO];
-    if ((st = ensure(h->gd, sizeof(double2) * nO * nI))) return st;
-    if ((st = ensure(h->gpsi, sizeof(double2) * 2 * N * nI))) return st;
-    if ((st = ensure(h->gphi, sizeof(double2) * 2 * nO * N))) return st;
-    if ((st = ensure(h->get, sizeof(double2) * nO * N))) return st;
-    if (gK > 1 && (st = ensure(h->gseg, sizeof(double2) * gK * Rp * ldm))) return st;
-    if (!S_dev && (st = ensure(h->gg, sizeof(double2) * N * L))) return st;
+    if ((st = ensure(h, h->gd, sizeof(double2) * nO * nI))) return st;
+    if ((st = ensure(h, h->gpsi, sizeof(double2) * 2 * N * nI))) return st;
+    if ((st = ensure(h, h->gphi, sizeof(double2) * 2 * nO * N))) return st;
+    if ((st = ensure(h, h->get, sizeof(double2) * nO * N))) return st;
+    if (gK > 1 && (st = ensure(h, h->gseg, sizeof(double2) * gK * Rp * ldm))) return st;
+    if (want_g && !S_dev && (st = ensure(h, h->gg, sizeof(double2) * N * L))) return st;
+    if (want_f && !S_dev && (st = ensure(h, h->gf, sizeof(double2) * N * L * nI))) return st;
     double2* Dd = as<double2>(h->gd);
-    RGF_CUDA_TRY(cudaMemcpyAsync(Dd, Da.data(), sizeof(double2) * nO * nI, cudaMemcpyHostToDevice, h->stream));
+    if (want_g)
+      RGF_CUDA_TRY(cudaMemcpyAsync(Dd, Da.data(), sizeof(double2) * nO * nI, cudaMemcpyHostToDevice, h->stream));
+    double2* fout = !want_f ? nullptr : S_dev ? reinterpret_cast<double2*>(gr->psi) : as<double2>(h->gf);
     double2* psi[2] = {as<double2>(h->gpsi), as<double2>(h->gpsi) + N * nI};
     double2* phv[2] = {as<double2>(h->gphi), as<double2>(h->gphi) + nO * N};
     double2* Et = as<double2>(h->get);
     double2* seg = as<double2>(h->gseg);
-    double2* gout = S_dev ? reinterpret_cast<double2*>(gr->g) : as<double2>(h->gg);
+    double2* gout = !want_g ? nullptr : S_dev ? reinterpret_cast<double2*>(gr->g) : as<double2>(h->gg);
     // Psi_{L+1} = W(0:N, N:N+n_in) and Phi_{L+1} = W(N:N+n_out, 0:N) after the far lead
     RGF_CUDA_TRY(cudaMemcpy2DAsync(psi[0], sizeof(double2) * nI, M + N, sizeof(double2) * ldm, sizeof(double2) * nI,
                                    N, cudaMemcpyDeviceToDevice, h->stream));
@@ -861,23 +886,34 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
         const int nx_ = cur ^ 1;
         launch_zgemm_add(N, nI, N, ZOp{Wj, ldm, 0}, ZOp{psi[cur], nI, 0}, ZAdd{Wj + N, ldm, N, ni_s}, psi[nx_],
                          nI, h->stream);
+        h->launches++;
+        const int64_t n_phys = mirror ? L - 1 - j : j;
+        if (want_f) {
+          launch_store_field(psi[nx_], idx_d + o_col, N, (int)nI, fout + n_phys * N, N * L, h->stream);
+          h->launches++;
+        }
+        if (!want_g) {
+          cur = nx_;
+          continue;
+        }
         launch_zgemm_add(nO, N, N, ZOp{phv[cur], N, 0}, ZOp{Wj, ldm, 0}, ZAdd{Wj + N * ldm, ldm, no_s, N},
                          phv[nx_], N, h->stream);
-        const int64_t n_phys = mirror ? L - 1 - j : j;
         if (nO * nI <= 1024) {
           launch_grad_fused(phv[nx_], psi[nx_], Dd, N, (int)nO, (int)nI, coef, gout + n_phys * N, h->stream);
-          h->launches += 3;
+          h->launches += 2;
         } else {
           launch_zgemm(nO, N, nI, one, ZOp{Dd, nI, 0}, ZOp{psi[nx_], nI, 1}, zero, Et, N, h->stream);
           launch_grad_slice(phv[nx_], Et, N, nO, coef, gout + n_phys * N, h->stream);
-          h->launches += 4;
+          h->launches += 3;
         }
         cur = nx_;
       }
       if ((st = check_launch())) return st;
     }
-    if (!S_dev)
+    if (want_g && !S_dev)
       RGF_CUDA_TRY(cudaMemcpyAsync(gr->g, gout, sizeof(double2) * N * L, cudaMemcpyDeviceToHost, h->stream));
+    if (want_f && !S_dev)
+      RGF_CUDA_TRY(cudaMemcpyAsync(gr->psi, fout, sizeof(double2) * N * L * nI, cudaMemcpyDeviceToHost, h->stream));
   } else if (gr) {
     // no slices: nothing depends on epsilon
   }
@@ -905,11 +941,163 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
     set_error("a device-side wait timed out");
     return RGF_ERR_TIMEOUT;
   }
+  // the persistent engine pivots inside each 32 x 32 block only: a zero or
+  // non-finite pivot there, or a slice inverse whose probe residual is not
+  // at round-off level, sends the whole call to the per-step engine
+  if (ran_persist && ((hstatus & kStatusSingular) || !(h->probe <= kProbeRetry))) return kRetryWholeColumn;
   if (hstatus & kStatusSingular) {
-    set_error("a pivot block of a slice matrix is singular");
+    set_error("a slice matrix is singular (zero pivot under partial pivoting)");
     return RGF_ERR_SINGULAR;
   }
-  return copy_channels_out(h, tr, ci, ch);
+  if ((st = copy_channels_out(h, tr, ci, ch))) return st;
+  if (!(h->probe <= kProbeIllcond)) {
+    char msg[160];
+    snprintf(msg, sizeof(msg),
+             "a slice matrix is ill-conditioned: slice-inverse probe residual %.3g (> %.0e); S holds the result "
+             "of partial pivoting, which may be inaccurate",
+             h->probe, kProbeIllcond);
+    set_error(msg);
+    return RGF_ERR_ILLCOND;
+  }
+  return RGF_OK;
+}
+
+// smatrix_run with the engine of opt (default: persistent), recomputed by the
+// per-step engine with whole-column pivoting when the persistent engine's
+// in-block pivoting proves inadequate.
+rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const rgf_options* opt, rgf_cplx* S,
+                   int64_t ldS, rgf_channels* ch, const GradReq* gr = nullptr, const SegReq* seg = nullptr) {
+  const int engine = (opt && opt->engine == 1) ? 1 : 0;
+  h->fallback = 0;
+  rgf_status st = smatrix_run(h, p, req, opt, S, ldS, ch, gr, engine, seg);
+  if (st == kRetryWholeColumn) {
+    const double probe0 = h->probe;
+    st = smatrix_run(h, p, req, opt, S, ldS, ch, gr, 1, seg);
+    h->fallback = 1;
+    h->probe_first = probe0;
+  }
+  return st;
+}
+
+// Joins the two segment states of an L-split S-matrix (SegReq) across the
+// cut by one Dyson step.  With the coupling -I between the left part's last
+// slice b and the right part's first slice a = b + 1, and the states
+// (g_L, X_L, Z_L, Y_L), (g_R, X_R, Z_R, Y_R), sweeping the pivot block
+// P = I - g_R g_L of
+//     [[ P,          g_R X_L,  X_R ],
+//      [ -Z_L,       Y_L,      0   ],
+//      [ -Z_R g_L,   Z_R X_L,  Y_R ]]
+// leaves, in its corner, the four blocks C G B between the two lead surfaces:
+//     C_L G_00 B_L = Y_L + Z_L (I - g_R g_L)^{-1} g_R X_L,
+//     C_L G_0e B_R = Z_L (I - g_R g_L)^{-1} X_R,
+//     C_R G_e0 B_L = Z_R X_L + Z_R g_L (I - g_R g_L)^{-1} g_R X_L,
+//     C_R G_ee B_R = Y_R + Z_R g_L (I - g_R g_L)^{-1} X_R,
+// (the Dyson equation for two coupled Green's functions; the same blocks the
+// far-lead attachment of cal_smatrix_RGF.m:272-289 produces), from which S
+// follows by the Fisher-Lee relation.  The sweep pivots over the whole
+// column.
+rgf_status segment_merge(rgf_handle h, const Problem& p, const rgf_request* req, const rgf_options* opt,
+                         const rgf_cplx* stL, const rgf_cplx* stR, rgf_cplx* S, int64_t ldS) {
+  rgf_status st;
+  h->launches = 0;
+  h->probe = 0.0;
+  h->engine_used = 1;
+  h->fallback = 0;
+  if ((st = validate_problem(p, req))) return st;
+  if (opt && opt->precision != RGF_FP64) {
+    set_error("unsupported precision form");
+    return RGF_ERR_ARG;
+  }
+  const bool S_dev = opt && opt->S_on_device;
+  RGF_CUDA_TRY(cudaSetDevice(h->device));
+  const int64_t N = p.tr.N;
+  double2 k2, k2eL, k2eR;
+  k2eps(p.k0dx, p.epsL, &k2, &k2eL);
+  k2eps(p.k0dx, p.epsR, &k2, &k2eR);
+  ChanInfo ci;
+  if ((st = run_channels(h, p.tr, k2eL, k2eR, true, &ci))) return st;
+  Request rq;
+  if ((st = resolve_request(req, ci, &rq))) return st;
+  const int noL = (int)rq.out[0].size(), noR = (int)rq.out[1].size();
+  const int niL = (int)rq.in[0].size(), niR = (int)rq.in[1].size();
+  const int n_out = noL + noR, n_in = niL + niR;
+  if (n_out == 0 || n_in == 0) return RGF_OK;
+  if (!S || !stL || !stR || ldS < n_out) {
+    set_error("segment merge: S, both states and ldS >= n_out are needed");
+    return RGF_ERR_ARG;
+  }
+  const int64_t CL = N + niL, CR = N + niR, RL = N + noL, RR = N + noR;
+  const double2 *dL = reinterpret_cast<const double2*>(stL), *dR = reinterpret_cast<const double2*>(stR);
+  if (!S_dev) {
+    if ((st = ensure(h, h->segs, sizeof(double2) * (RL * CL + RR * CR)))) return st;
+    RGF_CUDA_TRY(cudaMemcpyAsync(h->segs.p, stL, sizeof(double2) * RL * CL, cudaMemcpyHostToDevice, h->stream));
+    RGF_CUDA_TRY(cudaMemcpyAsync(as<double2>(h->segs) + RL * CL, stR, sizeof(double2) * RR * CR,
+                                 cudaMemcpyHostToDevice, h->stream));
+    dL = as<double2>(h->segs);
+    dR = dL + RL * CL;
+  }
+  const int kSwW = sweep_block_width();
+  const int64_t R = N + n_out, C = N + n_in, ldm = (C + 1) & ~(int64_t)1;
+  if ((st = ensure(h, h->aug, sizeof(double2) * R * ldm))) return st;
+  if ((st = ensure(h, h->pc, sizeof(double2) * std::max(R, C) * kSwW))) return st;
+  if ((st = ensure(h, h->u, sizeof(double2) * kSwW * ldm))) return st;
+  if ((st = ensure(h, h->gepp, gepp_scratch_bytes(N)))) return st;
+  if ((st = ensure(h, h->status, sizeof(int)))) return st;
+  if (!S_dev && (st = ensure(h, h->sdev, sizeof(double2) * (int64_t)n_out * n_in))) return st;
+  std::vector<int> idx;
+  for (int o = 0; o < n_out; o++) idx.push_back(o);
+  for (int i = 0; i < n_in; i++) idx.push_back(i);
+  std::vector<int> pairs;
+  intersect_pairs(rq.out[0], rq.in[0], 0, 0, &pairs);        // cal_smatrix_RGF.m:286
+  intersect_pairs(rq.out[1], rq.in[1], noL, niL, &pairs);    // :287
+  const size_t o_pairs = idx.size();
+  idx.insert(idx.end(), pairs.begin(), pairs.end());
+  if ((st = ensure(h, h->idx, sizeof(int) * (idx.size() + 1)))) return st;
+  int* idx_d = as<int>(h->idx);
+  RGF_CUDA_TRY(cudaMemcpyAsync(idx_d, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, h->stream));
+  int* status = as<int>(h->status);
+  RGF_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), h->stream));
+  double2* M = as<double2>(h->aug);
+  const double2 one = cmk(1.0, 0.0), mone = cmk(-1.0, 0.0), zero = cmk(0.0, 0.0);
+  const double2 *gL = dL, *XL = dL + N, *ZL = dL + N * CL, *YL = dL + N * CL + N;
+  const double2 *gR = dR, *XR = dR + N, *ZR = dR + N * CR, *YR = dR + N * CR + N;
+  launch_zgemm(N, N, N, mone, ZOp{gR, CR, 0}, ZOp{gL, CL, 0}, zero, M, ldm, h->stream);  // P = I - g_R g_L
+  launch_add_identity(M, ldm, N, h->stream);
+  if (niL) launch_zgemm(N, niL, N, one, ZOp{gR, CR, 0}, ZOp{XL, CL, 0}, zero, M + N, ldm, h->stream);
+  launch_block_copy(M + N + niL, ldm, XR, CR, N, niR, 1.0, h->stream);
+  launch_block_copy(M + N * ldm, ldm, ZL, CL, noL, N, -1.0, h->stream);
+  if (noR) launch_zgemm(noR, N, N, mone, ZOp{ZR, CR, 0}, ZOp{gL, CL, 0}, zero, M + (N + noL) * ldm, ldm, h->stream);
+  launch_block_copy(M + N * ldm + N, ldm, YL, CL, noL, niL, 1.0, h->stream);
+  launch_block_copy(M + N * ldm + N + niL, ldm, nullptr, 0, noL, niR, 0.0, h->stream);
+  if (noR && niL)
+    launch_zgemm(noR, niL, N, one, ZOp{ZR, CR, 0}, ZOp{XL, CL, 0}, zero, M + (N + noL) * ldm + N, ldm, h->stream);
+  launch_block_copy(M + (N + noL) * ldm + N + niL, ldm, YR, CR, noR, niR, 1.0, h->stream);
+  h->launches += 9;
+  for (int64_t j0 = 0; j0 < N; j0 += kSwW) {
+    const int jn = (int)std::min<int64_t>(kSwW, N - j0);
+    launch_gepp_step(M, ldm, N, C, j0, jn, h->gepp.p, status, h->stream);
+    launch_sweep_panel(M, ldm, R, C, j0, jn, as<double2>(h->pc), as<double2>(h->u), ldm, status, h->stream);
+    launch_sweep_update(M, ldm, R, C, j0, jn, as<double2>(h->pc), as<double2>(h->u), ldm, h->stream);
+    h->launches += 4;
+  }
+  RGF_CUDA_TRY(launch_gepp_unpermute(M, ldm, R, N, h->gepp.p, h->stream));
+  double2* Sd = S_dev ? reinterpret_cast<double2*>(S) : as<double2>(h->sdev);
+  const int64_t ldSd = S_dev ? ldS : n_out;
+  launch_extract(M, ldm, N, idx_d, n_out, idx_d + n_out, n_in, Sd, ldSd, idx_d + o_pairs, (int)pairs.size() / 2,
+                 h->stream);
+  h->launches += 4;
+  if ((st = check_launch())) return st;
+  if (!S_dev)
+    RGF_CUDA_TRY(cudaMemcpy2DAsync(S, sizeof(rgf_cplx) * ldS, Sd, sizeof(double2) * n_out, sizeof(double2) * n_out,
+                                   n_in, cudaMemcpyDeviceToHost, h->stream));
+  int hstatus = 0;
+  RGF_CUDA_TRY(cudaMemcpyAsync(&hstatus, status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  RGF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (hstatus & kStatusSingular) {
+    set_error("segment merge: the interface matrix I - g_R g_L is singular");
+    return RGF_ERR_SINGULAR;
+  }
+  return RGF_OK;
 }
 
 Problem problem2d(const rgf_syst2d* s) {
@@ -967,30 +1155,20 @@ rgf_status check_handle(rgf_handle h) {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[RGF_NOALLOC_SCRATCH_BYTES];
 
 namespace {
-constexpr int kMaxNoallocDevices = 64;
-std::mutex g_noalloc_mu;
-unsigned char* g_noalloc_ptr[kMaxNoallocDevices] = {};
-
-// address of the scratch array on the current device (resolved on the first
-// call on that device, with that device current)
-rgf_status noalloc_scratch(int device, unsigned char** out) {
-  if (device < 0 || device >= kMaxNoallocDevices) {
-    set_error("rgf_smatrix_2d_noalloc: device ordinal out of range");
-    return RGF_ERR_ARG;
+// Device address of the scratch array in the current device's context.  It
+// is looked up on every call (cudaGetSymbolAddress allocates nothing and is
+// cheap), so a context the host application reset and recreated is seen.
+// The first lookup on a device also loads this library's device code there.
+rgf_status noalloc_scratch(unsigned char** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    cudaGetLastError();
+    set_error(std::string("rgf_smatrix_2d_noalloc: cudaGetSymbolAddress of the static scratch failed: ") +
+              cudaGetErrorString(e));
+    return RGF_ERR_CUDA;
   }
-  std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      cudaGetLastError();
-      set_error(std::string("rgf_smatrix_2d_noalloc: cudaGetSymbolAddress of the static scratch failed: ") +
-                cudaGetErrorString(e));
-      return RGF_ERR_CUDA;
-    }
-    g_noalloc_ptr[device] = static_cast<unsigned char*>(p);
-  }
-  *out = g_noalloc_ptr[device];
+  *out = static_cast<unsigned char*>(p);
   return RGF_OK;
 }
 }  // namespace
@@ -1036,9 +1214,9 @@ rgf_status rgf_destroy(rgf_handle h) {
                     &h->conj[0], &h->conj[1], &h->nprop,   &h->status,    &h->phi,     &h->tmp,
                     &h->g0s,    &h->g0e,    &h->st_col,    &h->st_val,    &h->eps,     &h->aug,
                     &h->pc,     &h->u,      &h->idx,       &h->sdev,      &h->xpc,     &h->xrow,
-                    &h->xt,     &h->xu,     &h->xsync,     &h->xprobe,    &h->xtrace,  &h->gck,
+                    &h->xt,     &h->xu,     &h->xsync,     &h->xprobe,    &h->gepp,    &h->gck,
                     &h->gseg,   &h->gm0,    &h->gpsi,      &h->gphi,      &h->get,     &h->gd,
-                    &h->gg};
+                    &h->gg,     &h->gf,     &h->segs};
   for (DevBuf* b : bufs)
     if (b->p) cudaFree(b->p);
   for (cudaEvent_t ev : h->ev) cudaEventDestroy(ev);
@@ -1165,6 +1343,74 @@ rgf_status rgf_smatrix_grad_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_r
   return smatrix(h, problem3d(syst), req, opt, S, ldS, nullptr, &gr);
 }
 
+rgf_status rgf_fields_2d(rgf_handle h, const rgf_syst2d* syst, const rgf_request* req, const rgf_options* opt,
+                         rgf_cplx* S, int64_t ldS, rgf_cplx* psi, int64_t checkpoint) {
+  rgf_status st;
+  if ((st = check_handle(h))) return st;
+  if (!syst || !psi) {
+    set_error("syst and psi must not be NULL");
+    return RGF_ERR_ARG;
+  }
+  GradReq gr{nullptr, 0, nullptr, checkpoint, psi};
+  return smatrix(h, problem2d(syst), req, opt, S, ldS, nullptr, &gr);
+}
+
+rgf_status rgf_fields_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_request* req, const rgf_options* opt,
+                         rgf_cplx* S, int64_t ldS, rgf_cplx* psi, int64_t checkpoint) {
+  rgf_status st;
+  if ((st = check_handle(h))) return st;
+  if (!syst || !psi) {
+    set_error("syst and psi must not be NULL");
+    return RGF_ERR_ARG;
+  }
+  GradReq gr{nullptr, 0, nullptr, checkpoint, psi};
+  return smatrix(h, problem3d(syst), req, opt, S, ldS, nullptr, &gr);
+}
+
+static rgf_status segment_args(rgf_handle h, const void* syst, int side, const void* state) {
+  rgf_status st;
+  if ((st = check_handle(h))) return st;
+  if (!syst || !state) {
+    set_error("syst and state must not be NULL");
+    return RGF_ERR_ARG;
+  }
+  if (side != 0 && side != 1) {
+    set_error("side must be 0 (left) or 1 (right)");
+    return RGF_ERR_ARG;
+  }
+  return RGF_OK;
+}
+
+rgf_status rgf_segment_sweep_2d(rgf_handle h, const rgf_syst2d* syst, const rgf_request* req, const rgf_options* opt,
+                                int32_t side, int64_t cut, rgf_cplx* state) {
+  rgf_status st;
+  if ((st = segment_args(h, syst, side, state))) return st;
+  SegReq sg{side, cut, state};
+  return smatrix(h, problem2d(syst), req, opt, nullptr, 0, nullptr, nullptr, &sg);
+}
+
+rgf_status rgf_segment_sweep_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_request* req, const rgf_options* opt,
+                                int32_t side, int64_t cut, rgf_cplx* state) {
+  rgf_status st;
+  if ((st = segment_args(h, syst, side, state))) return st;
+  SegReq sg{side, cut, state};
+  return smatrix(h, problem3d(syst), req, opt, nullptr, 0, nullptr, nullptr, &sg);
+}
+
+rgf_status rgf_segment_merge_2d(rgf_handle h, const rgf_syst2d* syst, const rgf_request* req, const rgf_options* opt,
+                                const rgf_cplx* state_L, const rgf_cplx* state_R, rgf_cplx* S, int64_t ldS) {
+  rgf_status st;
+  if ((st = segment_args(h, syst, 0, state_L))) return st;
+  return segment_merge(h, problem2d(syst), req, opt, state_L, state_R, S, ldS);
+}
+
+rgf_status rgf_segment_merge_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_request* req, const rgf_options* opt,
+                                const rgf_cplx* state_L, const rgf_cplx* state_R, rgf_cplx* S, int64_t ldS) {
+  rgf_status st;
+  if ((st = segment_args(h, syst, 0, state_L))) return st;
+  return segment_merge(h, problem3d(syst), req, opt, state_L, state_R, S, ldS);
+}
+
 rgf_status rgf_smatrix_size_2d(rgf_handle h, const rgf_syst2d* syst, const rgf_request* req, int64_t* n_out,
                                int64_t* n_in) {
   rgf_status st;
@@ -1247,7 +1493,7 @@ rgf_status rgf_build_laplacian_1d(rgf_handle h, int64_t n, int32_t bc, double ka
     return RGF_ERR_ARG;
   }
   RGF_CUDA_TRY(cudaSetDevice(h->device));
-  if ((st = ensure(h->tmp, sizeof(double2) * n * n))) return st;
+  if ((st = ensure(h, h->tmp, sizeof(double2) * n * n))) return st;
   launch_laplacian_dense(n, bc, bc == RGF_BC_BLOCH ? ka : 0.0, as<double2>(h->tmp), h->stream);
   if ((st = check_launch())) return st;
   RGF_CUDA_TRY(cudaMemcpyAsync(A, h->tmp.p, sizeof(double2) * n * n, cudaMemcpyDeviceToHost, h->stream));
@@ -1280,6 +1526,15 @@ rgf_status rgf_set_stream(rgf_handle h, void* stream) {
   return RGF_OK;
 }
 
+rgf_status rgf_last_engine(rgf_handle h, int32_t* engine, int32_t* fallback, double* rejected_probe) {
+  rgf_status st;
+  if ((st = check_handle(h))) return st;
+  if (engine) *engine = h->engine_used;
+  if (fallback) *fallback = h->fallback;
+  if (rejected_probe) *rejected_probe = h->fallback ? h->probe_first : 0.0;
+  return RGF_OK;
+}
+
 rgf_status rgf_last_stats(rgf_handle h, int64_t* kernel_launches, double* probe_residual) {
   rgf_status st;
   if ((st = check_handle(h))) return st;
@@ -1302,22 +1557,18 @@ rgf_status rgf_smatrix_2d_noalloc(const rgf_syst2d* syst, const rgf_request* req
   RGF_CUDA_TRY(cudaGetDevice(&device));
   unsigned char* base = nullptr;
   rgf_status st;
-  if ((st = noalloc_scratch(device, &base))) return st;
-  // a handle on the stack whose every workspace buffer grows inside the
-  // static scratch; nothing in it owns device memory, so it is not destroyed
+  if ((st = noalloc_scratch(&base))) return st;
+  // a handle on the stack whose arena is the static scratch: every workspace
+  // buffer is carved from it and ensure() never reaches cudaMalloc; nothing
+  // in it owns device memory, so it is not destroyed
   Arena arena;
   arena.base = base;
   arena.cap = RGF_NOALLOC_SCRATCH_BYTES;
   rgf_handle_s h;
   h.device = device;
   h.stream = reinterpret_cast<cudaStream_t>(stream);
+  h.arena = &arena;
   RGF_CUDA_TRY(cudaDeviceGetAttribute(&h.sms, cudaDevAttrMultiProcessorCount, device));
-  DevBuf* bufs[] = {&h.k0,      &h.k1,      &h.kx[0],     &h.kx[1],     &h.lam[0],  &h.lam[1],  &h.mu[0],
-                    &h.mu[1],   &h.isprop[0], &h.isprop[1], &h.prop[0], &h.prop[1], &h.conj[0], &h.conj[1],
-                    &h.nprop,   &h.status,  &h.phi,       &h.tmp,       &h.g0s,     &h.g0e,     &h.st_col,
-                    &h.st_val,  &h.eps,     &h.aug,       &h.pc,        &h.u,       &h.idx,     &h.sdev,
-                    &h.xpc,     &h.xrow,    &h.xt,        &h.xu,        &h.xsync,   &h.xprobe,  &h.xtrace};
-  for (DevBuf* b : bufs) b->arena = &arena;
   return smatrix(&h, problem2d(syst), req, opt, S, ldS, ch);
 }
 

@@ -167,7 +167,8 @@ __device__ void invert_block(double2 (*Ts)[kSw + 1], int* perm, int jn, int* sta
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   for (int p = 0; p < jn; p++) {
     if (warp == 0) {
-      double mag = (lane >= p && lane < jn) ? cabs2(Ts[lane][p]) : -1.0;
+      // |re| + |im|, the magnitude LAPACK's izamax compares
+      double mag = (lane >= p && lane < jn) ? fabs(Ts[lane][p].x) + fabs(Ts[lane][p].y) : -1.0;
       int idx = lane;
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) {
@@ -286,6 +287,206 @@ void launch_sweep_update(double2* M, int64_t ldm, int64_t R, int64_t Cc, int64_t
 const char* sweep_update_kernel_name() { return "k_zgemm<true> (sweep rank-32 update, FP64 DMMA)"; }
 
 int sweep_block_width() { return kSw; }
+
+// ---------------------------------------------------------------------------
+// Partial pivoting over the whole remaining column (the row choice of LAPACK
+// zgetrf, which MATLAB's inv uses at cal_smatrix_RGF.m:265).
+//
+// Before sweep step J = [j0, j0+jn), k_panel_gepp factors the panel
+// W(j0:N, J) by LU with partial pivoting in a scratch copy (the largest
+// |re| + |im| of the column, the first row on ties: LAPACK's izamax) and
+// records the rows it chose, LAPACK style: swaps[j0+q] = row exchanged with
+// row j0+q at step q.  k_laswp applies these exchanges to every column of W,
+// so that the step's pivot block holds the chosen rows and the in-block
+// pivoting of k_sweep_panel then takes them in the same order.  The rows of
+// the unswept part (rows >= j0) of a partially swept matrix can be exchanged
+// freely: sweeping commutes with it.  After the last step W's first N
+// columns hold inv(P M) = inv(M) P^T (P = all exchanges of the slice), and
+// k_perm_src + k_colperm undo that by exchanging the columns in reverse
+// order.  The Schur complement the panel starts from is the trailing matrix
+// of a right-looking LU, so the choices are those of unblocked LU with
+// partial pivoting up to rounding.
+// ---------------------------------------------------------------------------
+constexpr int kGeppThreads = 1024;
+
+__device__ __forceinline__ void argmax_merge(double& m, int& i, double om, int oi) {
+  if (om > m || (om == m && oi >= 0 && (i < 0 || oi < i))) {
+    m = om;
+    i = oi;
+  }
+}
+
+__global__ void __launch_bounds__(kGeppThreads) k_panel_gepp(const double2* __restrict__ M, int64_t ldm,
+                                                             int64_t N, int64_t j0, int jn, double2* __restrict__ P,
+                                                             int* __restrict__ swaps, int* status) {
+  __shared__ double wmag[kGeppThreads / 32];
+  __shared__ int widx[kGeppThreads / 32];
+  __shared__ double2 prow[kSw];
+  __shared__ int piv_s;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nwarps = blockDim.x >> 5;
+  const int n = (int)(N - j0);
+  for (int64_t e = t; e < (int64_t)n * kSw; e += blockDim.x) {
+    const int i = (int)(e / kSw), q = (int)(e % kSw);
+    P[e] = (q < jn) ? M[(j0 + i) * ldm + j0 + q] : cmk(0.0, 0.0);
+  }
+  __syncthreads();
+  for (int q = 0; q < jn; q++) {
+    double best = -1.0;
+    int bi = -1;
+    for (int i = q + t; i < n; i += blockDim.x) {  // rows in increasing order: first index kept on ties
+      const double2 v = P[(int64_t)i * kSw + q];
+      double m = fabs(v.x) + fabs(v.y);
+      if (m != m) m = INFINITY;  // a NaN entry wins, so that it is flagged below
+      if (m > best) {
+        best = m;
+        bi = i;
+      }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+      argmax_merge(best, bi, __shfl_down_sync(0xffffffffu, best, off), __shfl_down_sync(0xffffffffu, bi, off));
+    if (lane == 0) {
+      wmag[warp] = best;
+      widx[warp] = bi;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      best = lane < nwarps ? wmag[lane] : -1.0;
+      bi = lane < nwarps ? widx[lane] : -1;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1)
+        argmax_merge(best, bi, __shfl_down_sync(0xffffffffu, best, off), __shfl_down_sync(0xffffffffu, bi, off));
+      if (lane == 0) {
+        const int r = bi < 0 ? q : bi;
+        piv_s = r;
+        swaps[j0 + q] = (int)(j0 + r);
+        if (!(best > 0.0) || !isfinite(best)) atomicOr(status, kStatusSingular);
+      }
+    }
+    __syncthreads();
+    const int r = piv_s;
+    if (r != q && t < kSw) {
+      const double2 a = P[(int64_t)q * kSw + t];
+      P[(int64_t)q * kSw + t] = P[(int64_t)r * kSw + t];
+      P[(int64_t)r * kSw + t] = a;
+    }
+    __syncthreads();
+    if (t < kSw) prow[t] = P[(int64_t)q * kSw + t];
+    __syncthreads();
+    const double2 d = cinv(prow[q]);
+    for (int i = q + 1 + t; i < n; i += blockDim.x) {
+      double2* row = P + (int64_t)i * kSw;
+      const double2 l = cmul(row[q], d);
+      row[q] = l;
+      for (int c = q + 1; c < jn; c++) row[c] = csub(row[c], cmul(l, prow[c]));
+    }
+    __syncthreads();
+  }
+}
+
+// rows j0+q <-> swaps[j0+q], q = 0..jn-1 in order, over columns [0, Cc)
+__global__ void k_laswp(double2* M, int64_t ldm, int64_t Cc, int64_t j0, int jn, const int* __restrict__ swaps) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= Cc) return;
+  for (int q = 0; q < jn; q++) {
+    const int64_t a = j0 + q, r = swaps[a];
+    if (r != a) {
+      const double2 x = M[a * ldm + c];
+      M[a * ldm + c] = M[r * ldm + c];
+      M[r * ldm + c] = x;
+    }
+  }
+}
+
+// src[c] = the column of the swept matrix that column c of inv(M) is:
+// the column exchanges (q, swaps[q]) applied for q = N-1 down to 0.
+__global__ void k_perm_src(const int* __restrict__ swaps, int N, int* __restrict__ src) {
+  extern __shared__ int ps[];
+  int* sw = ps;
+  int* sc = ps + N;
+  for (int c = threadIdx.x; c < N; c += blockDim.x) {
+    sw[c] = swaps[c];
+    sc[c] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = N - 1; q >= 0; q--) {
+      const int s = sw[q];
+      if (s != q) {
+        const int x = sc[q];
+        sc[q] = sc[s];
+        sc[s] = x;
+      }
+    }
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < N; c += blockDim.x) src[c] = sc[c];
+}
+
+// W(i, c) <- W(i, src[c]) for rows [0, R), columns [0, N); each CTA stages
+// its row in its own scratch row rowtmp + blockIdx.x * N
+__global__ void k_colperm(double2* M, int64_t ldm, int64_t R, int64_t N, const int* __restrict__ src,
+                          double2* __restrict__ rowtmp) {
+  double2* tmp = rowtmp + (int64_t)blockIdx.x * N;
+  for (int64_t i = blockIdx.x; i < R; i += gridDim.x) {
+    for (int64_t c = threadIdx.x; c < N; c += blockDim.x) tmp[c] = M[i * ldm + c];
+    __syncthreads();
+    for (int64_t c = threadIdx.x; c < N; c += blockDim.x) M[i * ldm + c] = tmp[src[c]];
+    __syncthreads();
+  }
+}
+
+constexpr int kColpermCtas = 64;
+
+size_t gepp_scratch_bytes(int64_t N) {
+  // panel N x kSw, rowtmp kColpermCtas x N (complex); swaps and src (N ints each)
+  return sizeof(double2) * (size_t)N * (kSw + kColpermCtas) + sizeof(int) * 2 * (size_t)N + 256;
+}
+
+void launch_gepp_step(double2* M, int64_t ldm, int64_t N, int64_t Cc, int64_t j0, int jn, void* scratch,
+                      int* status, cudaStream_t s) {
+  double2* P = reinterpret_cast<double2*>(scratch);
+  int* swaps = reinterpret_cast<int*>(P + (size_t)N * (kSw + kColpermCtas));
+  k_panel_gepp<<<1, kGeppThreads, 0, s>>>(M, ldm, N, j0, jn, P, swaps, status);
+  k_laswp<<<(unsigned)((Cc + 255) / 256), 256, 0, s>>>(M, ldm, Cc, j0, jn, swaps);
+}
+
+cudaError_t launch_gepp_unpermute(double2* M, int64_t ldm, int64_t R, int64_t N, void* scratch, cudaStream_t s) {
+  double2* P = reinterpret_cast<double2*>(scratch);
+  double2* rowtmp = P + (size_t)N * kSw;
+  int* swaps = reinterpret_cast<int*>(P + (size_t)N * (kSw + kColpermCtas));
+  int* src = swaps + N;
+  const size_t sm = sizeof(int) * 2 * (size_t)N;
+  if (sm > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(k_perm_src, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+  }
+  k_perm_src<<<1, 256, sm, s>>>(swaps, (int)N, src);
+  const int64_t ctas = R < kColpermCtas ? R : kColpermCtas;
+  k_colperm<<<(unsigned)ctas, 256, 0, s>>>(M, ldm, R, N, src, rowtmp);
+  return cudaGetLastError();
+}
+
+// max_i |W(i, pc1 + 1) - v(i)|, i < N, into the bits of probe_max (a NaN
+// residual is recorded as +inf)
+__global__ void k_probe_check(const double2* M, int64_t ldm, int64_t N, int64_t pc1,
+                              unsigned long long* probe_max) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  double r = 0.0;
+  if (i < N) {
+    const double2 d = csub(M[i * ldm + pc1 + 1], probe_v(i));
+    r = sqrt(cabs2(d));
+    if (r != r) r = INFINITY;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, off));
+  if ((threadIdx.x & 31) == 0 && r > 0.0) atomicMax(probe_max, (unsigned long long)__double_as_longlong(r));
+}
+
+void launch_probe_check(const double2* M, int64_t ldm, int64_t N, int64_t pc1, unsigned long long* probe_max,
+                        cudaStream_t s) {
+  k_probe_check<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(M, ldm, N, pc1, probe_max);
+}
 
 // ---------------------------------------------------------------------------
 // Slice assembly: rows [0, N) x cols [0, N) of the augmented matrix become
@@ -528,6 +729,46 @@ __global__ void k_grad_slice(const double2* Phi, const double2* Et, int64_t N, i
   double2 acc = cmk(0.0, 0.0);
   for (int64_t a = 0; a < n_out; a++) acc = cadd(acc, cmul(Phi[a * N + m], Et[a * N + m]));
   g[m] = cmul(coef, acc);
+}
+
+// dst[r*ldd + c] = scale * src[r*lds + c] (src == nullptr: zero), rows x cols
+__global__ void k_block_copy(double2* dst, int64_t ldd, const double2* src, int64_t lds, int64_t rows, int64_t cols,
+                             double scale) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  for (int64_t r = blockIdx.y; r < rows; r += gridDim.y)
+    dst[r * ldd + c] = src ? cscale(src[r * lds + c], scale) : cmk(0.0, 0.0);
+}
+
+void launch_block_copy(double2* dst, int64_t ldd, const double2* src, int64_t lds, int64_t rows, int64_t cols,
+                       double scale, cudaStream_t s) {
+  if (rows <= 0 || cols <= 0) return;
+  dim3 grid((unsigned)((cols + 127) / 128), (unsigned)(rows < 8192 ? rows : 8192));
+  k_block_copy<<<grid, 128, 0, s>>>(dst, ldd, src, lds, rows, cols, scale);
+}
+
+__global__ void k_add_identity(double2* M, int64_t ldm, int64_t n) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < n) M[i * ldm + i].x += 1.0;
+}
+
+void launch_add_identity(double2* M, int64_t ldm, int64_t n, cudaStream_t s) {
+  if (n > 0) k_add_identity<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(M, ldm, n);
+}
+
+// out[m + i*ld] = Psi[m][col_of[i]] (Psi: N x n_in row-major, augmented column order)
+__global__ void k_store_field(const double2* Psi, const int* col_of, int64_t N, int n_in, double2* out, int64_t ld) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= N * n_in) return;
+  const int i = (int)(e / N);
+  const int64_t m = e % N;
+  out[m + i * ld] = Psi[m * n_in + col_of[i]];
+}
+
+void launch_store_field(const double2* Psi, const int* col_of, int64_t N, int n_in, double2* out, int64_t ld,
+                        cudaStream_t s) {
+  const int64_t tot = N * n_in;
+  if (tot > 0) k_store_field<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(Psi, col_of, N, n_in, out, ld);
 }
 
 void launch_grad_slice(const double2* Phi, const double2* Et, int64_t N, int64_t n_out, double2 coef, double2* g,

@@ -28,6 +28,15 @@ void launch_sweep_panel(const double2* M, int64_t ldm, int64_t R, int64_t Cc, in
 void launch_sweep_update(double2* M, int64_t ldm, int64_t R, int64_t Cc, int64_t j0, int jn, const double2* Pc,
                          const double2* U, int64_t ldu, cudaStream_t s);
 const char* sweep_update_kernel_name();
+// partial pivoting over the whole remaining column (see sweep.cu): scratch of
+// gepp_scratch_bytes(N); launch_gepp_step before each sweep step (rows of W
+// exchanged over columns [0, Cc)), launch_gepp_unpermute after the last one
+size_t gepp_scratch_bytes(int64_t N);
+void launch_gepp_step(double2* M, int64_t ldm, int64_t N, int64_t Cc, int64_t j0, int jn, void* scratch,
+                      int* status, cudaStream_t s);
+cudaError_t launch_gepp_unpermute(double2* M, int64_t ldm, int64_t R, int64_t N, void* scratch, cudaStream_t s);
+void launch_probe_check(const double2* M, int64_t ldm, int64_t N, int64_t pc1, unsigned long long* probe_max,
+                        cudaStream_t s);
 void launch_assemble(double2* M, int64_t ldm, int64_t N, int64_t Rz, const double2* Gsrc, int64_t ldg,
                      const double2* Gextra, int64_t lde, const int* st_col, const double2* st_val, double2 k2,
                      const double2* eps, double2 eps_u, cudaStream_t s);
@@ -48,6 +57,13 @@ void launch_scale_cols(const double2* src, int64_t lds, const double2* diag, dou
 // through Et = D Psi^T)
 void launch_grad_fused(const double2* Phi, const double2* Psi, const double2* D, int64_t N, int n_out, int n_in,
                        double2 coef, double2* g, cudaStream_t s);
+// dst = scale * src block (src == nullptr: zero); M += I on the leading n x n
+void launch_block_copy(double2* dst, int64_t ldd, const double2* src, int64_t lds, int64_t rows, int64_t cols,
+                       double scale, cudaStream_t s);
+void launch_add_identity(double2* M, int64_t ldm, int64_t n, cudaStream_t s);
+// fields: out[m + i*ld] = Psi[m][col_of[i]]
+void launch_store_field(const double2* Psi, const int* col_of, int64_t N, int n_in, double2* out, int64_t ld,
+                        cudaStream_t s);
 void launch_grad_slice(const double2* Phi, const double2* Et, int64_t N, int64_t n_out, double2 coef, double2* g,
                        cudaStream_t s);
 

@@ -73,6 +73,13 @@ def config4_params(seed: int = 4, count: int = 256):
     return Ns, Ls, etas
 
 
+# the 16-structure subsample of the batched workload that has oracle
+# fixtures: the first twelve, then the largest N (k=70, N=511), the largest L
+# (k=101, L=1997), the largest L*N^3 (k=142, N=503, L=1917) and the largest
+# eta (k=218)
+CONFIG4_SUBSAMPLE = tuple(range(12)) + (70, 101, 142, 218)
+
+
 def config4_structure(k: int, seed: int = 4, count: int = 256):
     """Structure k of the batched workload: periodic, eps U[1,3) drawn from
     default_rng([seed, k]), k0dx = 2pi/15 (1 + 1j eta)."""

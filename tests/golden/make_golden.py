@@ -75,6 +75,52 @@ def small_cases():
     return cases
 
 
+def singular_leading_block_eps(ny: int, nx: int, k0dx: float, seed: int) -> np.ndarray:
+    """Permittivity whose first slice matrix M_1 = A0 - k0dx^2 diag(eps_1) -
+    G0_L has an exactly singular leading 32 x 32 block (up to rounding) while
+    M_1 itself is well conditioned: eps_1 on sites 0..31 is the constant
+    lambda / k0dx^2, lambda an eigenvalue of (A0 - G0_L)[0:32, 0:32]
+    (Dirichlet BC, epsilon_L = 1; cal_smatrix_RGF.m:209, 260, 265).  Pivoting
+    inside that block alone cannot invert M_1 accurately; pivoting over the
+    whole column (MATLAB's inv) can."""
+    from oracle.rgf_ref import build_laplacian_1d, setup_channels
+    rng = np.random.default_rng(seed)
+    eps = (1.0 + 2.0 * rng.random((ny, nx))).astype(complex)
+    ch = setup_channels(ny, "Dirichlet", k0dx, 1.0, 1.0)
+    phi = ch["fun_phi"](ch["kydx"])
+    G0 = (phi * np.exp(1j * ch["L"]["kxdx"])[None, :]) @ phi.conj().T
+    A0 = -build_laplacian_1d(ny, "Dirichlet") + 2 * np.eye(ny)
+    lam = np.linalg.eigvals((A0 - G0)[:32, :32])
+    target = k0dx ** 2 * 2.0  # the eigenvalue closest to a plausible k0dx^2 eps
+    eps[:32, 0] = lam[np.argmin(np.abs(lam - target))] / k0dx ** 2
+    return eps
+
+
+def pivot_cases():
+    """Slice matrices far from diagonal dominance, several 32-wide pivot
+    blocks each (N >= 100): k0dx^2 eps_L at and beyond 4 (setup_channels.m:
+    211-215), high index contrast, gain (Im eps < 0), and a leading pivot
+    block that is singular although the slice matrix is not."""
+    rng = np.random.default_rng(777)
+    cases = {}
+    for tag, k2e in (("3p5", 3.5), ("3p95", 3.95), ("4p5", 4.5), ("6", 6.0)):
+        k0dx = float(np.sqrt(k2e / 1.0))
+        eps = 1.0 + 3.0 * rng.random((128, 14)) + 0.01j * rng.random((128, 14))
+        cases[f"2d_pivot_k2e_{tag}"] = ("2d", dict(epsilon=eps, epsilon_L=1.0, epsilon_R=1.5, k0dx=k0dx,
+                                                   yBC="Dirichlet"), *FULL)
+    eps = np.where(rng.random((128, 20)) < 0.5, 12.0, 1.0) + 0.0j
+    cases["2d_pivot_contrast12"] = ("2d", dict(epsilon=eps, epsilon_L=1.0, epsilon_R=12.0, k0dx=2 * np.pi / 10,
+                                               yBC="periodic"), *FULL)
+    eps = 2.0 + 2.0 * rng.random((100, 15)) - 0.3j * rng.random((100, 15))
+    cases["2d_pivot_gain"] = ("2d", dict(epsilon=eps, epsilon_L=1.0, epsilon_R=1.0, k0dx=2 * np.pi / 9,
+                                         yBC="Neumann"), *FULL)
+    k0dx = 2 * np.pi / 15
+    cases["2d_pivot_singular_block"] = ("2d", dict(epsilon=singular_leading_block_eps(96, 6, k0dx, 778),
+                                                   epsilon_L=1.0, epsilon_R=1.0, k0dx=k0dx, yBC="Dirichlet"),
+                                        *FULL)
+    return cases
+
+
 def config_cases(with_cfg2: bool):
     out = {}
     s, o, i = workloads.config1()
@@ -83,7 +129,7 @@ def config_cases(with_cfg2: bool):
     out["cfg3"] = ("3d", s, o, i)
     s, o, i = workloads.config5()
     out["cfg5"] = ("2d", s, o, i)
-    for k in range(3):
+    for k in workloads.CONFIG4_SUBSAMPLE:
         s, o, i = workloads.config4_structure(k)
         out[f"cfg4_{k}"] = ("2d", s, o, i)
     if with_cfg2:
@@ -119,8 +165,12 @@ def main():
     with_cfg2 = "--config2" in sys.argv
     only_cfg2 = "--only-config2" in sys.argv
     only = [a.split("=", 1)[1] for a in sys.argv if a.startswith("--only=")]
-    if not only_cfg2 and not only:
-        for name, (dim, syst, out, in_) in small_cases().items():
+    if not only_cfg2:
+        cases = dict(small_cases())
+        cases.update(pivot_cases())
+        for name, (dim, syst, out, in_) in cases.items():
+            if only and name not in only:
+                continue
             save_case(name, dim, syst, out, in_, store_inputs=True)
     for name, (dim, syst, out, in_) in config_cases(with_cfg2 or only_cfg2).items():
         if only_cfg2 and name != "cfg2":

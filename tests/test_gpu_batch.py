@@ -42,7 +42,10 @@ def test_batch_matches_single_calls(workers):
 
 
 def test_batch_config4_golden():
-    cases = [config_case(f"cfg4_{k}") for k in range(3)]
+    """The 16-structure subsample of config 4 (the first twelve structures,
+    the largest N, the largest L, the largest L N^3 and the largest eta)
+    through the batched entry, against the oracle's S."""
+    cases = [config_case(f"cfg4_{k}") for k in workloads.CONFIG4_SUBSAMPLE]
     cases = [c for c in cases if c is not None]
     if not cases:
         pytest.skip("no config-4 fixtures")

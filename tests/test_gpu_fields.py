@@ -1,0 +1,77 @@
+"""Fields inside the structure (rgf_fields_2d/3d through the C ABI) against a
+dense solve of the whole block-tridiagonal operator (oracle/dense_fdfd.py):
+psi[:, n, b] = G_{n, s(b)} B_b for every slice n and requested input b, for
+every request form, both engines and several checkpoint intervals.
+
+Tolerance: max |psi - psi_dense| <= 1e-11 max |psi_dense| (FP64 throughout)."""
+import numpy as np
+import pytest
+
+import rgf_b200
+from oracle.dense_fdfd import fields_dense_2d
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-11
+
+
+def relmax(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+CASES = [
+    ("periodic", ["left", "right"], ["left", "right"]),
+    ("Dirichlet", {"ind_out_R": [1, 2]}, {"ind_in_L": [2, 1]}),
+    ("Neumann", ["left"], ["left"]),
+    (0.4, ["right"], ["right"]),
+    ("DirichletNeumann", ["left", "right"], ["right"]),
+]
+
+
+@pytest.mark.parametrize("engine", [0, 1])
+@pytest.mark.parametrize("ckpt", [0, 3])
+@pytest.mark.parametrize("bc,out,inp", CASES)
+def test_fields_match_dense_solve(bc, out, inp, engine, ckpt):
+    rng = np.random.default_rng(12)
+    syst = dict(epsilon=1 + 2 * rng.random((9, 7)) + 0.02j * rng.random((9, 7)), epsilon_L=1.0, epsilon_R=1.4,
+                k0dx=1.1, yBC=bc)
+    S, psi = rgf_b200.fields_RGF(syst, out, inp, checkpoint=ckpt, options={"engine": engine})
+    S0, psi0 = fields_dense_2d(syst, out, inp)
+    assert np.linalg.norm(S - S0) <= 1e-11 * np.linalg.norm(S0)
+    assert psi.shape == psi0.shape
+    assert relmax(psi, psi0) <= TOL
+
+
+def test_fields_multiblock():
+    """N > 32 (several pivot blocks) and the persistent engine."""
+    rng = np.random.default_rng(13)
+    syst = dict(epsilon=1 + 3 * rng.random((70, 11)), epsilon_L=1.0, epsilon_R=1.0, k0dx=2 * np.pi / 15,
+                yBC="periodic")
+    S, psi = rgf_b200.fields_RGF(syst, ["left", "right"], {"ind_in_L": [1, 3], "ind_in_R": [2]})
+    S0, psi0 = fields_dense_2d(syst, ["left", "right"], {"ind_in_L": [1, 3], "ind_in_R": [2]})
+    assert relmax(psi, psi0) <= TOL
+
+
+def test_fields_energy_flux_real_eps():
+    """A homogeneous slab (eps = eps_L = 1): the field of channel b is the
+    lead's own propagating mode, psi[:, n, b] = G0-propagated profile with
+    |psi| constant along the slab (no reflection)."""
+    syst = dict(epsilon=np.ones((16, 10)), epsilon_L=1.0, epsilon_R=1.0, k0dx=2 * np.pi / 8, yBC="periodic")
+    _, psi = rgf_b200.fields_RGF(syst, ["right"], {"ind_in_L": [1]})
+    amp = np.linalg.norm(psi[:, :, 0], axis=0)
+    assert np.abs(amp - amp[0]).max() <= 1e-12 * amp[0]
+
+
+def test_fields_3d_consistent_with_2d():
+    """3D with a size-1 x axis and periodic BC is the 2D problem (the n = 1
+    Laplacian is zero)."""
+    rng = np.random.default_rng(14)
+    eps2 = 1 + 2 * rng.random((8, 6))
+    s2 = dict(epsilon=eps2, epsilon_L=1.0, epsilon_R=1.0, k0dx=1.0, yBC="periodic")
+    s3 = dict(epsilon=eps2[None, :, :], epsilon_L=1.0, epsilon_R=1.0, k0dx=1.0, xyBC="periodic")
+    S2, p2 = rgf_b200.fields_RGF(s2, ["left", "right"], ["left"])
+    S3, p3 = rgf_b200.fields_RGF_3D(s3, ["left", "right"], ["left"])
+    assert p3.shape == (1, 8, 6, p2.shape[2])
+    # channel order may differ between the 2D and 3D set-ups: compare the
+    # field space spanned by the inputs through S's unitary structure
+    assert np.linalg.norm(S3) == pytest.approx(np.linalg.norm(S2), rel=1e-12)
+    assert np.linalg.norm(p3) == pytest.approx(np.linalg.norm(p2), rel=1e-11)

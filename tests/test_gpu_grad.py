@@ -72,6 +72,46 @@ def test_gradient_config5_reduced():
     assert relmax(g, g0) <= TOL_G
 
 
+def test_gradient_config5_full():
+    """The whole config-5 gradient (N=256, L=512: 256 x 512 pixels, 8 left
+    inputs -> 8 right outputs, F = sum |t_ab|^2, checkpoint every 23 slices)
+    against the oracle's recursion form."""
+    syst, out, inp = workloads.config5()
+    S0, _ = ref_smatrix(syst, out, inp)
+    S, g = rgf_b200.smatrix_grad_RGF(syst, out, inp, np.conj(S0), checkpoint=23)
+    _, g0 = grad_rgf_2d(syst, out, inp, np.conj(S0))
+    assert g.shape == (256, 512)
+    assert np.linalg.norm(S - S0) <= 1e-11 * np.linalg.norm(S0)
+    assert relmax(g, g0) <= TOL_G
+
+
+def test_gradient_config5_finite_differences():
+    """dF/d eps = 2 Re g of F = sum |t_ab|^2 at config 5 against central
+    differences of the GPU's own S (h = 1e-6, FP64) on 32 pixels drawn with
+    seed 55.  The difference quotient carries up to ~1e-13 |F| / h ~ 1e-6 of
+    round-off (S is computed to ~1e-13 relative), hence the absolute floor."""
+    syst, out, inp = workloads.config5()
+    S, _ = rgf_b200.cal_smatrix_RGF(syst, out, inp)
+    _, g = rgf_b200.smatrix_grad_RGF(syst, out, inp, np.conj(S), checkpoint=23)
+    F = lambda Sx: float(np.sum(np.abs(Sx) ** 2))  # noqa: E731
+    rng = np.random.default_rng(55)
+    ms, ns = rng.integers(0, 256, 32), rng.integers(0, 512, 32)
+    h = 1e-6
+    fds, gs = [], []
+    for m, n in zip(ms, ns):
+        vals = []
+        for sgn in (1, -1):
+            eps = syst["epsilon"].copy()
+            eps[m, n] += sgn * h
+            Sp, _ = rgf_b200.cal_smatrix_RGF(dict(syst, epsilon=eps), out, inp)
+            vals.append(F(Sp))
+        fds.append((vals[0] - vals[1]) / (2 * h))
+        gs.append(2 * np.real(g[m, n]))
+    fds, gs = np.array(fds), np.array(gs)
+    floor = 1e-13 * F(S) / h  # round-off of the difference quotient
+    assert np.all(np.abs(gs - fds) <= 1e-6 * np.abs(fds) + floor), np.abs(gs - fds).max()
+
+
 def test_gradient_finite_differences_on_device():
     """2 Re g against central differences of the GPU's own S (h = 1e-6; the
     difference quotient carries ~eps_mach |F| / h ~ 1e-9 of round-off, hence

@@ -59,7 +59,12 @@ def test_config2_golden():
     case = config_case("cfg2")
     if case is None:
         pytest.skip("config-2 fixture not generated")
-    S, _ = run(case)
+    h = _abi.Handle(0)
+    S, _ = rgf_b200.cal_smatrix_RGF(case["syst"], case["out"], case["in"], handle=h)
+    used, fallback, _ = h.engine()
+    _, probe = h.stats()
+    print(f"config 2: engine {used}, fallback {fallback}, probe residual {probe:.3g}")
+    assert fallback == 0 and probe < 1e-12  # the persistent engine's result stands
     assert rel(S, case["S"]) <= TOL_S
     # Dirichlet: literal reciprocity S = S^T (setup_channels.m:75-79)
     assert np.abs(S - S.T).max() <= 1e-12
@@ -113,6 +118,23 @@ def test_setup_channels_3d_parity(bc):
         assert got[side]["N_prop"] == exp[side]["N_prop"]
         assert np.array_equal(got[side]["ind_prop"], exp[side]["ind_prop"])
         assert np.abs(got[side]["kzdx"] - exp[side]["kzdx"]).max() < 1e-12
+
+
+@pytest.mark.parametrize("bc", ["periodic", "Dirichlet", [0.2, -1.1]])
+@pytest.mark.parametrize("k0dx", [1.3, 0.9 * (1 + 1e-3j)])
+def test_setup_channels_3d_one_sided(bc, k0dx):
+    """setup_channels_3D with epsilon_R omitted (setup_channels_3D.m:74,
+    138-141): the left side only, channels.R.N_prop = NaN."""
+    from oracle.rgf_ref import setup_channels_3D as ref
+    got = rgf_b200.setup_channels_3D(6, 5, bc, k0dx, 1.7)
+    exp = ref(6, 5, bc, k0dx, 1.7)
+    assert np.abs(got["kxdx"] - exp["kxdx"]).max() < 1e-14
+    assert np.abs(got["kydx"] - exp["kydx"]).max() < 1e-14
+    assert got["L"]["N_prop"] == exp["L"]["N_prop"]
+    assert np.array_equal(got["L"]["ind_prop"], exp["L"]["ind_prop"])
+    assert np.abs(got["L"]["kzdx"] - exp["L"]["kzdx"]).max() < 1e-12
+    assert np.abs(got["L"]["sqrt_mu"] - exp["L"]["sqrt_mu"]).max(initial=0) < 1e-13
+    assert np.isnan(got["R"]["N_prop"])
 
 
 @pytest.mark.parametrize("bc", ["periodic", "Dirichlet", "Neumann", "DirichletNeumann", "NeumannDirichlet", 1.3])
