@@ -46,6 +46,7 @@ METRIC = "S-matrices/s 2D N=1024 L=4096: 3xTF32+refine vs FP64 at 1e-10 rel err;
 UNIT = "S-matrices/s"
 FP64_DMMA_FALLBACK_TFLOPS = 37.0  # earlier measurement on this pool, used only if the live one fails
 PROFILE_EVERY = 64
+REF_ARM_SLICES = 32  # slices the reference arm samples per timed step
 DRAM_BYTES_PER_SLICE = (20.995072e6 + 8.149248e6) / 16  # k_persist<96,96>, config 2, ncu over 16 slices
 
 
@@ -181,9 +182,11 @@ def run_reference(args, dist):
     from rgf_b200 import workloads
     syst, out, in_ = workloads.config2()
     cores = os.cpu_count()
+    # each timed step samples REF_ARM_SLICES slices (K steps sample K times as
+    # many in all); warm-up steps sample 4
     vals = []
     for i in range(args.warmup + args.steps):
-        v, per_slice, setup = cpu_oracle_rate(syst, out, in_, args.ref_slices)
+        v, per_slice, setup = cpu_oracle_rate(syst, out, in_, REF_ARM_SLICES if i >= args.warmup else 4)
         if i >= args.warmup:
             vals.append(v)
     value = statistics.mean(vals)
@@ -194,7 +197,8 @@ def run_reference(args, dist):
             "config": config_dict(),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": f"numpy/scipy FP64 restatement of cal_smatrix_RGF.m (MATLAB not installed): "
-                                       f"{args.ref_slices} of 4096 slices + lead set-up per step, "
+                                       f"{REF_ARM_SLICES} of 4096 slices + lead set-up per timed step "
+                                       f"({REF_ARM_SLICES * args.steps} slices in all), "
                                        f"extrapolated linearly in L; OpenBLAS threads={cores}"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -268,11 +272,11 @@ def grad_over_fwd(h, dev, stream, reps: int = 5):
                         "F = sum|t|^2, checkpoint every 23 slices"}
 
 
-def batch_rate(dev, count: int = 32, workers: int = 8):
-    """Config-4 batched form: the first `count` of the 256 seeded structures
-    (N uniform 64..512, L uniform 100..2000, eps 1+2U, complex k0dx), full S
-    each, through rgf_smatrix_batch_2d with host inputs and outputs; timed by
-    the host around the blocking call (warm-up call first)."""
+def batch_rate(dev, count: int = 256, workers: int = 8):
+    """Config-4 batched form: all 256 seeded structures (N uniform 64..512,
+    L uniform 100..2000, eps 1+2U, complex k0dx), full S each, through
+    rgf_smatrix_batch_2d with host inputs and outputs; timed by the host
+    around the blocking call (warm-up call on four structures first)."""
     import rgf_b200
     from rgf_b200 import workloads
     items = [workloads.config4_structure(k) for k in range(count)]
@@ -367,7 +371,8 @@ def run_ours(args, dist):
     torch.cuda.synchronize()
     dist.barrier()
     t_ms, prof = timed(True, args.steps, PROFILE_EVERY)
-    launches, _ = h.stats()
+    launches, probe = h.stats()  # of the last timed call
+    used, fallback, _ = h.engine()
     torch.cuda.synchronize()
     dist.barrier()
     clk = clocks.stop()
@@ -396,14 +401,17 @@ def run_ours(args, dist):
     n, ms, fl_exec, name = prof
     fl = nx * workloads.canonical_slice_flops(ny, n_in // 2, n_out // 2)  # the launch covers all nx slices
     achieved = fl / (ms / n / 1e3) / 1e12 if n else None
-    # DRAM bytes (read + write) of one k_persist launch: the ncu capture of the
-    # first 16 slices (profiles/k_persist_config2_16slices.md) scaled to the
-    # launch's slice count (the traffic per slice is constant)
+    # DRAM bytes (read + write) of one k_persist launch: an ncu capture of the
+    # first 16 slices of this workload scaled to the launch's slice count (the
+    # traffic per slice is constant); a constant of this script, not measured
+    # in this run
     traffic = DRAM_BYTES_PER_SLICE * nx
     line["roofline"] = {"bound": "tensor", "kernel": name, "achieved": achieved, "peak": peak,
                         "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
                         "traffic": traffic, "flops_per_launch": fl, "executed_flops_per_launch": fl_exec,
-                        "timed_launches": n, "peak_source": peak_source}
+                        "timed_launches": n, "peak_source": peak_source,
+                        "traffic_source": "constant: ncu dram__bytes_read.sum + dram__bytes_write.sum of "
+                                          "k_persist<96,96> over the first 16 slices of this workload, x 4096/16"}
     line["e2e"] = {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(eps_host.numel() * 16),
                    "d2h_bytes_per_step": int(n_out * n_in * 16)}
     line["gpu_launches"] = int(launches) * args.steps
@@ -416,6 +424,8 @@ def run_ours(args, dist):
         S0 = np.load(gpath, allow_pickle=True)["S"]
         line["rel_err_vs_oracle"] = float(np.linalg.norm(S - S0) / np.linalg.norm(S0))
     line["reciprocity_err"] = float(np.abs(S - S.T).max())
+    line["slice_check"] = {"probe_residual": probe, "engine": "persistent (in-block pivoting)" if used == 0 else
+                           "per-step (whole-column pivoting)", "recomputed": bool(fallback)}
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count()
         v, per_slice, setup = cpu_oracle_rate(syst, out, in_, args.ref_slices)
@@ -435,7 +445,7 @@ def main():
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--ref-slices", type=int, default=32)
+    ap.add_argument("--ref-slices", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--slices", type=int, default=0,
                     help="profiling only: keep the first n slices (the JSON line is then not a bench number)")

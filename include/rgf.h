@@ -272,6 +272,14 @@ RGF_API rgf_status rgf_last_engine(rgf_handle h, int32_t* engine, int32_t* fallb
  * the algorithmic flops of one such launch, and its name. */
 RGF_API rgf_status rgf_last_profile(rgf_handle h, int64_t* timed_launches, double* total_ms,
                                     double* flops_per_launch, char* kernel_name, size_t name_len);
+/* Tuned tile shapes of the persistent engine (an addition): a matrix of Rp
+ * active rows (N plus the output channels carried) uses the square tile
+ * tile[i] (32, 64 or 96) of the first entry with Rp <= rows_max[i] (rows_max
+ * non-decreasing) whenever its grid fits the GPU, else the built-in choice
+ * (the largest tile that keeps >= 60% of the SMs busy).  n = 0 clears the
+ * table.  Batched calls pass it to their pipelines.  rgf_b200.autotune writes
+ * such a table from timed sweeps and caches it as JSON. */
+RGF_API rgf_status rgf_set_tile_table(rgf_handle h, int32_t n, const int64_t* rows_max, const int32_t* tile);
 /* Issue all work of this handle on the caller's stream (a cudaStream_t);
  * NULL restores the handle's own stream. */
 RGF_API rgf_status rgf_set_stream(rgf_handle h, void* stream);

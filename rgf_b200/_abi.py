@@ -26,6 +26,7 @@ BC_PERIODIC, BC_DIRICHLET, BC_NEUMANN, BC_DIRICHLET_NEUMANN, BC_NEUMANN_DIRICHLE
 RGF_ALL = -1
 RGF_FP64 = 0
 RGF_NOALLOC_SCRATCH_BYTES = 32 << 20  # include/rgf.h
+RGF_NOALLOC_SCRATCH_BYTES = 32 << 20  # include/rgf.h
 
 
 class Cplx(ctypes.Structure):
@@ -106,6 +107,7 @@ SIGNATURES = {
     "rgf_last_profile": (c_int, [c_void_p, POINTER(c_int64), POINTER(c_double), POINTER(c_double), c_char_p,
                                  ctypes.c_size_t]),
     "rgf_set_stream": (c_int, [c_void_p, c_void_p]),
+    "rgf_set_tile_table": (c_int, [c_void_p, c_int32, c_void_p, c_void_p]),
     "rgf_smatrix_2d_noalloc": (c_int, [POINTER(Syst2D), POINTER(Request), POINTER(Options), c_void_p, c_int64,
                                        POINTER(Channels), c_void_p]),
 }

@@ -72,6 +72,10 @@ struct rgf_handle_s {
   std::string prof_kernel;
   double probe = 0.0;
   DevBuf gepp;  // scratch of the whole-column pivoting (per-step engine)
+  // tuned tile table of the persistent engine: rows Rp <= tile_rmax[i] use
+  // tile tile_bm[i] (first match) when its grid fits the GPU
+  std::vector<int64_t> tile_rmax;
+  std::vector<int> tile_bm;
   int engine_used = 0;     // engine of the last call's final run
   int fallback = 0;        // 1: the persistent engine's result was rejected and recomputed
   double probe_first = 0;  // probe residual of the rejected run
@@ -107,10 +111,12 @@ rgf_status ensure(rgf_handle h, DevBuf& b, size_t bytes) {
     a->used += need;
     return RGF_OK;
   }
-  if (b.p) cudaFree(b.p);
+  // stream-ordered (re)allocation: cudaFree / cudaMalloc would synchronize the
+  // whole device, stalling the concurrent pipelines of a batched call
+  if (b.p) cudaFreeAsync(b.p, h->stream);
   b.p = nullptr;
   b.bytes = 0;
-  cudaError_t e = cudaMalloc(&b.p, bytes);
+  cudaError_t e = cudaMallocAsync(&b.p, bytes, h->stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
     set_error(std::string("device allocation of ") + std::to_string(bytes) + " bytes failed: " +
@@ -636,8 +642,19 @@ rgf_status smatrix_run(rgf_handle h, const Problem& p, const rgf_request* req, c
     return RGF_OK;
   };
   int BMp = 0, BNp = 0;
-  bool use_persist =
-      L > 0 && engine == 0 && persist_choose_tile(Rp, Cp, h->sms, &BMp, &BNp, h->sm_budget != nullptr);
+  auto choose_tile = [&]() {
+    for (size_t q = 0; q < h->tile_rmax.size(); q++) {
+      if (Rp > h->tile_rmax[q]) continue;
+      const int t = h->tile_bm[q];
+      if (((Rp + t - 1) / t) * ((Cp + t - 1) / t) + kPersistExtraCtas <= h->sms) {
+        BMp = BNp = t;
+        return true;
+      }
+      break;
+    }
+    return persist_choose_tile(Rp, Cp, h->sms, &BMp, &BNp, h->sm_budget != nullptr);
+  };
+  bool use_persist = L > 0 && engine == 0 && choose_tile();
   bool ran_persist = false;
   // per-slice probe residual (both engines)
   unsigned long long* probe_d = nullptr;
@@ -1278,6 +1295,8 @@ rgf_status rgf_smatrix_batch_2d(rgf_handle h, int64_t count, const rgf_syst2d* s
   for (int i = 0; i < nw; i++) {
     h->workers[i]->sms = h->sms;
     h->workers[i]->sm_budget = &h->sm_free;
+    h->workers[i]->tile_rmax = h->tile_rmax;
+    h->workers[i]->tile_bm = h->tile_bm;
   }
   // largest first (sum over slices of N^3 + N^2 P), so that the pipelines finish together
   std::vector<int64_t> order(count);
@@ -1523,6 +1542,28 @@ rgf_status rgf_set_stream(rgf_handle h, void* stream) {
   rgf_status st;
   if ((st = check_handle(h))) return st;
   h->stream = stream ? reinterpret_cast<cudaStream_t>(stream) : h->own_stream;
+  return RGF_OK;
+}
+
+rgf_status rgf_set_tile_table(rgf_handle h, int32_t n, const int64_t* rows_max, const int32_t* tile) {
+  rgf_status st;
+  if ((st = check_handle(h))) return st;
+  if (n < 0 || (n > 0 && (!rows_max || !tile))) {
+    set_error("tile table: n >= 0 and non-NULL arrays");
+    return RGF_ERR_ARG;
+  }
+  for (int32_t i = 0; i < n; i++) {
+    if (tile[i] != 32 && tile[i] != 64 && tile[i] != 96) {
+      set_error("tile table: tile must be 32, 64 or 96");
+      return RGF_ERR_ARG;
+    }
+    if (i > 0 && rows_max[i] < rows_max[i - 1]) {
+      set_error("tile table: rows_max must be non-decreasing");
+      return RGF_ERR_ARG;
+    }
+  }
+  h->tile_rmax.assign(rows_max, rows_max + n);
+  h->tile_bm.assign(tile, tile + n);
   return RGF_OK;
 }
 

@@ -139,3 +139,13 @@ def test_cpu_stand_ins_of_segments_and_fields_exist():
     st = segment_state_2d(s, ["left"], ["left"], 0, 1)
     assert st.shape[0] == 4 + S.shape[0] // 2 or st.shape[0] >= 4
     assert callable(segment_merge_2d)
+
+
+def test_constants_match_header():
+    src = open(HEADER).read()
+    m = re.search(r"#define RGF_NOALLOC_SCRATCH_BYTES \(\(size_t\)(\d+) << (\d+)\)", src)
+    assert m and int(m.group(1)) << int(m.group(2)) == _abi.RGF_NOALLOC_SCRATCH_BYTES
+    enum = dict(re.findall(r"^\s*(RGF_ERR_\w+|RGF_OK) = (\d+)", src, flags=re.M))
+    assert len(enum) == 9
+    for name, val in enum.items():
+        assert _abi.STATUS_NAMES[int(val)] == name

@@ -123,3 +123,57 @@ def test_noalloc_size_limit_is_the_documented_one():
 def _sizes_for(h, ny, req):
     sy, eps = problem(ny, 2, _abi.BC_PERIODIC, seed=ny)
     return s_size(h, sy, req)
+
+
+def noalloc_footprint_bytes(N, n_out, n_in, nx, eps_on_host=True, two_leads=False):
+    """The workspace of rgf_smatrix_2d_noalloc as include/rgf.h states it."""
+    R, C = N + n_out, N + n_in + 2
+    b = 16 * (3 * N * N + R * (C + 1) + 64 * R + 288 * C + 110 * N)
+    if two_leads:
+        b += 16 * N * N
+    if eps_on_host:
+        b += 16 * N * nx
+    return b
+
+
+def test_noalloc_size_limit_is_the_documented_one():
+    """The largest ny accepted for a full two-sided periodic S (epsilon on the
+    host, 2 slices), found by bisection, is the one the header's footprint
+    formula predicts (to 1%); ny + 1 is rejected, and ny matches the
+    allocating entry."""
+    lib = _abi.load()
+    h = _abi.Handle(0)
+    req, keep = _request(["left", "right"], ["left", "right"])
+    opt = _abi.Options(_abi.RGF_FP64, 0, 0, 0)
+
+    def attempt(ny):
+        sy, eps = problem(ny, 2, _abi.BC_PERIODIC, seed=ny)
+        no, ni = s_size(h, sy, req)
+        S = np.zeros((no, ni), dtype=complex, order="F")
+        st = lib.rgf_smatrix_2d_noalloc(ctypes.byref(sy), ctypes.byref(req), ctypes.byref(opt), S.ctypes.data, no,
+                                        None, None)
+        assert st in (_abi.RGF_OK, _abi.RGF_ERR_ARG), _abi.STATUS_NAMES.get(st, st)
+        return st == _abi.RGF_OK, (sy, eps, no, ni, S)
+
+    lo, hi = 300, 1200  # lo fits, hi does not
+    assert attempt(lo)[0] and not attempt(hi)[0]
+    while hi - lo > 1:
+        mid = (lo + hi) // 2
+        if attempt(mid)[0]:
+            lo = mid
+        else:
+            hi = mid
+    ok, (sy, eps, no, ni, S) = attempt(lo)
+    assert ok and not attempt(lo + 1)[0]
+    ref = np.zeros((no, ni), dtype=complex, order="F")
+    _abi.check(lib.rgf_smatrix_2d(h.h, ctypes.byref(sy), ctypes.byref(req), ctypes.byref(opt), ref.ctypes.data, no,
+                                  None))
+    assert rel(S, ref) <= TOL_S
+    sizes = {}
+    for n in range(lo - 30, lo + 31):
+        sy_n, eps_n = problem(n, 2, _abi.BC_PERIODIC, seed=n)
+        sizes[n] = s_size(h, sy_n, req)
+    pred = max(n for n, (no_n, ni_n) in sizes.items()
+               if noalloc_footprint_bytes(n, no_n, ni_n, nx=2) <= _abi.RGF_NOALLOC_SCRATCH_BYTES)
+    assert abs(pred - lo) <= 0.01 * lo, (pred, lo)
+    del keep
