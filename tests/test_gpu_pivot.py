@@ -48,7 +48,9 @@ def test_pivot_regime_matches_oracle(path, engine):
     assert rel(S, case["S"]) <= TOL_S
     used, fallback, _ = h.engine()
     _, probe = h.stats()
-    assert probe < 1e-10
+    # the residual scales with |G_n| |M_n|: at index contrast 12 it reaches
+    # ~2e-10 under whole-column pivoting while S still matches to 1e-11
+    assert probe < 1e-9
     if engine == 1:
         assert used == 1 and fallback == 0
 
