@@ -272,7 +272,7 @@ def grad_over_fwd(h, dev, stream, reps: int = 5):
                         "F = sum|t|^2, checkpoint every 23 slices"}
 
 
-def batch_rate(dev, count: int = 256, workers: int = 8):
+def batch_rate(dev, count: int = 256, workers: int = 16):
     """Config-4 batched form: all 256 seeded structures (N uniform 64..512,
     L uniform 100..2000, eps 1+2U, complex k0dx), full S each, through
     rgf_smatrix_batch_2d with host inputs and outputs; timed by the host

@@ -204,13 +204,35 @@ class Handle:
 _tls = threading.local()
 
 
-def default_handle(device: int = 0) -> Handle:
+def default_handle(device: int = 0, mode: str = "latency") -> Handle:
+    """This thread's handle on `device`, with the tuned tile table of this GPU
+    model (rgf_b200/tuned, written by rgf_b200.autotune) installed when there
+    is one: the fastest tiles for single S-matrices (mode "latency") or the
+    fewest SM-microseconds for batches (mode "throughput")."""
     hs = getattr(_tls, "handles", None)
     if hs is None:
         hs = _tls.handles = {}
-    if device not in hs:
-        hs[device] = Handle(device)
-    return hs[device]
+    key = (device, mode)
+    if key not in hs:
+        h = Handle(device)
+        _install_tuned(h, mode)
+        hs[key] = h
+    return hs[key]
+
+
+def _install_tuned(h: Handle, mode: str) -> None:
+    from . import autotune
+    # the table is keyed by the GPU model and SM count, read here from torch
+    # when it is importable
+    try:
+        import torch
+        p = torch.cuda.get_device_properties(h.device)
+        name, sms = p.name, p.multi_processor_count
+    except Exception:
+        return
+    table = autotune.load(name, sms)
+    if table:
+        autotune.install(h, table, mode)
 
 
 def ptr(a: np.ndarray) -> int:

@@ -291,7 +291,7 @@ def cal_smatrix_RGF_batch(systs, outs, ins, *, workers: int = 0, device: int = 0
         outs = [outs] * n
     if not isinstance(ins, (list, tuple)) or (ins and isinstance(ins[0], str)):
         ins = [ins] * n
-    h = handle or _abi.default_handle(device)
+    h = handle or _abi.default_handle(device, "throughput")
     keep, sy_list, rq_list, S_list = [], [], [], []
     for syst, out, in_ in zip(systs, outs, ins):
         _check_syst(syst, "yBC")

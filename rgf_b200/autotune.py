@@ -47,9 +47,30 @@ def table_from_measurements(rows: list) -> tuple:
     return rmax, tile
 
 
-def install(handle, table: dict) -> None:
-    """Install a tuned table (as written by ``tune``) on an _abi.Handle."""
-    rmax, tile = table_from_measurements(table["entries"])
+def grid_sms(rows: int, tile: int) -> int:
+    """SMs one persistent sweep of a full request holds: its tiles (Rp rows,
+    Rp + 2 columns rounded up to even) plus the T-server and prep CTAs."""
+    cols = ((rows + 1) & ~1) + 2
+    return -(-rows // tile) * -(-cols // tile) + 2
+
+
+def annotate(table: dict) -> dict:
+    """Adds to every entry the tile that needs the fewest SM-microseconds per
+    slice ("best_throughput": the choice when many structures share the GPU,
+    as in a batch) beside the fastest one ("best")."""
+    for e in table["entries"]:
+        cost = {int(t): us * grid_sms(e["rows"], int(t)) for t, us in e["us_per_slice"].items()}
+        e["sm_us_per_slice"] = {str(t): round(c, 1) for t, c in cost.items()}
+        e["best_throughput"] = min(cost, key=cost.get)
+    return table
+
+
+def install(handle, table: dict, mode: str = "latency") -> None:
+    """Install a tuned table (as written by ``tune``) on an _abi.Handle: the
+    fastest tile per size (mode "latency", single S-matrices) or the one with
+    the fewest SM-microseconds (mode "throughput", batches)."""
+    key = "best" if mode == "latency" else "best_throughput"
+    rmax, tile = table_from_measurements([{"rows": e["rows"], "best": e[key]} for e in table["entries"]])
     a = (ctypes.c_int64 * max(len(rmax), 1))(*rmax)
     b = (ctypes.c_int32 * max(len(tile), 1))(*tile)
     _abi.check(handle.lib.rgf_set_tile_table(handle.h, len(rmax), a, b))
@@ -114,9 +135,9 @@ def tune(device: int = 0, sizes=DEFAULT_SIZES, slices: int = 24, reps: int = 3) 
     _abi.check(lib.rgf_set_tile_table(h.h, 0, None, None))
     del keep
     h.close()
-    return {"gpu": props.name, "sms": props.multi_processor_count, "slices": slices,
-            "workload": "2D periodic, eps 1+2U, k0dx 2pi/15, full S", "time": time.strftime("%Y-%m-%d %H:%M:%S"),
-            "entries": entries}
+    return annotate({"gpu": props.name, "sms": props.multi_processor_count, "slices": slices,
+                     "workload": "2D periodic, eps 1+2U, k0dx 2pi/15, full S",
+                     "time": time.strftime("%Y-%m-%d %H:%M:%S"), "entries": entries})
 
 
 def main():

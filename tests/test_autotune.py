@@ -45,3 +45,19 @@ def test_tuning_run_and_installed_table():
                                         options=_abi.Options(_abi.RGF_FP64, 0, 0, 1))
         assert h.profile()[3].startswith(f"k_persist<{tile},")
         assert np.linalg.norm(S - S0) <= 1e-12 * np.linalg.norm(S0)
+
+
+def test_annotate_picks_fewest_sm_microseconds():
+    t = autotune.annotate({"entries": [{"N": 256, "rows": 291, "us_per_slice": {"96": 193.0, "64": 147.0, "32": 129.0},
+                                        "best": 32}]})
+    e = t["entries"][0]
+    assert e["best_throughput"] == 96  # 11 SMs x 193 us beats 27 x 147 and 102 x 129
+    assert autotune.grid_sms(291, 96) == 11 and autotune.grid_sms(291, 32) == 102
+
+
+def test_committed_b200_table():
+    """The table measured on this pool's B200s (148 SMs) is in the package."""
+    t = autotune.load("NVIDIA B200", 148)
+    assert t is not None and t["sms"] == 148 and len(t["entries"]) >= 8
+    for e in t["entries"]:
+        assert e["best"] in (32, 64, 96) and e["best_throughput"] in (32, 64, 96)
