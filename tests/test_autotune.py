@@ -51,8 +51,8 @@ def test_annotate_picks_fewest_sm_microseconds():
     t = autotune.annotate({"entries": [{"N": 256, "rows": 291, "us_per_slice": {"96": 193.0, "64": 147.0, "32": 129.0},
                                         "best": 32}]})
     e = t["entries"][0]
-    assert e["best_throughput"] == 96  # 11 SMs x 193 us beats 27 x 147 and 102 x 129
-    assert autotune.grid_sms(291, 96) == 11 and autotune.grid_sms(291, 32) == 102
+    assert e["best_throughput"] == 96  # 18 SMs x 193 us beats 27 x 147 and 102 x 129
+    assert autotune.grid_sms(291, 96) == 18 and autotune.grid_sms(291, 32) == 102
 
 
 def test_committed_b200_table():
