@@ -160,10 +160,14 @@ RGF_API rgf_status rgf_smatrix_3d(rgf_handle h, const rgf_syst3d* syst, const rg
 
 /* Batched form: `count` independent 2D problems (each as rgf_smatrix_2d:
  * systs[i], reqs[i], S[i] with leading dimension ldS[i]; all host or all
- * device per opt->S_on_device), run as `workers` concurrent pipelines (<= 0:
- * 8), each with its own stream and workspace inside the handle, largest
- * problems first.  The pipelines' persistent sweeps share the GPU's SMs
- * through one budget, so their cooperative grids are always co-resident.
+ * device per opt->S_on_device).  workers <= 0 (default): every structure's
+ * set-up runs on a host thread and stream of its own, and all their slice
+ * sweeps run in ONE persistent cooperative launch in which gangs of CTAs,
+ * sized to each structure, take the structures from a work queue in device
+ * memory, largest first (at most 256 structures per launch; a structure that
+ * needs tiles smaller than 96 x 96 sweeps on its own first).  workers > 0:
+ * that many concurrent pipelines (host threads, each with its own stream and
+ * workspace), whose persistent sweeps share the GPU's SMs through one budget.
  * statuses (may be NULL) receives each problem's status; the return value
  * is the first failure (message names the item).  The reference has no
  * batched call: its user loops over cal_smatrix_RGF. */

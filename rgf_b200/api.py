@@ -284,8 +284,10 @@ def cal_smatrix_RGF_3D(syst, out, in_, *, device: int = 0, options=None, handle=
 
 def cal_smatrix_RGF_batch(systs, outs, ins, *, workers: int = 0, device: int = 0, options=None, handle=None):
     """[S_1, ..., S_n] for n independent 2D structures (cal_smatrix_RGF on
-    each), computed as concurrent pipelines on the GPU; outs / ins are lists
-    (one request per structure) or a single request used for all."""
+    each); outs / ins are lists (one request per structure) or a single
+    request used for all.  workers = 0: all slice sweeps in one persistent
+    launch (gangs of CTAs sized to each structure from a device work queue);
+    workers > 0: that many concurrent pipelines."""
     n = len(systs)
     if not isinstance(outs, (list, tuple)) or (outs and isinstance(outs[0], str)):
         outs = [outs] * n

@@ -56,7 +56,7 @@ namespace {
 constexpr int kPB = 32;  // pivot block width
 constexpr int kPanelWarps = 4, kPanelThreads = kPanelWarps * 32;  // one warpgroup
 constexpr int kBarMath = 1, kBarPanel = 2, kBarPub = 3, kBarDjj = 4, kBarSrv = 5, kBarPre0 = 6,
-              kBarPre1 = 7, kBarSrv2 = 8;  // named barriers
+              kBarPre1 = 7, kBarSrv2 = 8, kBarGang = 9;  // named barriers
 constexpr int kMaxTile = 96;
 constexpr int kServerThreads = 256;  // the math warpgroups of the T-server CTA
 constexpr unsigned kFull = 0xffffffffu;
@@ -1277,9 +1277,159 @@ __global__ void __launch_bounds__(Cfg<BM, BN>::Threads, 1) k_persist(PersistPara
   }
 }
 
+// ---------------------------------------------------------------------------
+// Many structures in one launch: gangs of CTAs sized to each structure, handed
+// out by a work queue in device memory.
+// ---------------------------------------------------------------------------
+// The grid holds one CTA per SM.  A CTA that is free takes the queue's lock,
+// joins the pool of free CTAs and, while the structure at the head of the
+// queue (the items are ordered by cost, largest first) needs no more CTAs
+// than the pool holds, hands it a gang: each gang member gets the item and its
+// place in the item's grid (tile CTA, T-server or prep CTA) through its
+// mailbox.  Every member then runs the role the single-structure kernel would
+// give it, with the item's own exchange buffers and flags; when it returns,
+// the CTA is free again.  Once the queue is empty every CTA in the pool is
+// told to stop.  The head of the queue always fits the grid, so when all
+// gangs have finished it is dispatched: no deadlock.  Waits for the lock and
+// for a mailbox are bounded by `sched_timeout` cycles (they may span the run
+// of a whole structure) and poll the queue's abort word.
+__device__ __forceinline__ int ldcg_i(const int* p) { return __ldcg(p); }
+__device__ __forceinline__ void stcg_i(int* p, int v) { __stcg(p, v); }
+
+__device__ bool gang_lock(GangState* gs, long long timeout) {
+  const long long t0 = clock64();
+  while (atomicCAS(&gs->lock, 0, 1) != 0) {
+    if (ldcg_i(&gs->abort)) return false;
+    if (clock64() - t0 > timeout) {
+      atomicExch(&gs->abort, 1);
+      return false;
+    }
+    __nanosleep(64);
+  }
+  __threadfence();
+  return true;
+}
+
+__device__ void gang_unlock(GangState* gs) {
+  __threadfence();
+  atomicExch(&gs->lock, 0);
+}
+
+__device__ void gang_mail(GangState* gs, int cta, int item, int local) {
+  stcg_i(&gs->mail_item[cta], item);
+  stcg_i(&gs->mail_local[cta], local);
+  __threadfence();
+  atomicAdd(&gs->mail_seq[cta], 1);
+}
+
+// thread 0 of CTA `me`: the next assignment (item, place), item < 0 = stop
+__device__ void gang_next(const GangItem* items, int count, GangState* gs, int me, int seq, long long timeout,
+                          int* item, int* local) {
+  *item = -1;
+  *local = 0;
+  if (!gang_lock(gs, timeout)) return;
+  int nfree = ldcg_i(&gs->nfree);
+  int next = ldcg_i(&gs->next);
+  stcg_i(&gs->pool[nfree++], me);
+  while (next < count && items[next].ctas <= nfree) {
+    const int need = items[next].ctas;
+    for (int l = 0; l < need; l++) gang_mail(gs, ldcg_i(&gs->pool[--nfree]), next, l);
+    next++;
+  }
+  if (next >= count) {
+    while (nfree > 0) gang_mail(gs, ldcg_i(&gs->pool[--nfree]), -1, 0);
+  }
+  stcg_i(&gs->nfree, nfree);
+  stcg_i(&gs->next, next);
+  gang_unlock(gs);
+  const long long t0 = clock64();
+  for (int spins = 0;; spins++) {
+    if (ld_acquire(&gs->mail_seq[me]) > seq) break;
+    if (ldcg_i(&gs->abort)) return;
+    if ((spins & 63) == 63 && clock64() - t0 > timeout) {
+      atomicExch(&gs->abort, 1);
+      return;
+    }
+    __nanosleep(128);
+  }
+  *item = ldcg_i(&gs->mail_item[me]);
+  *local = ldcg_i(&gs->mail_local[me]);
+}
+
+template <int BM, int BN>
+__global__ void __launch_bounds__(Cfg<BM, BN>::Threads, 1)
+    k_persist_gang(const GangItem* __restrict__ items, int count, GangState* gs, long long sched_timeout) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Shared& sh = *reinterpret_cast<Shared*>(smem_raw);
+  __shared__ int s_item, s_local;
+  constexpr int kAll = Cfg<BM, BN>::Threads;
+  const uint32_t mb = smem_u32(&sh.mbar);
+  // The two warpgroup kinds keep their own loops (their register budgets
+  // differ after setmaxnreg) and meet only at the named barrier kBarGang.
+  if (threadIdx.x < Cfg<BM, BN>::MathThreads) {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(Cfg<BM, BN>::MathRegs));
+    if (threadIdx.x == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+    for (int seq = 0;; seq++) {
+      if (threadIdx.x == 0) {
+        int item, local;
+        gang_next(items, count, gs, (int)blockIdx.x, seq, sched_timeout, &item, &local);
+        s_item = item;
+        s_local = local;
+        if (item >= 0) {
+          // the mbarrier's phase restarts with the structure's step count
+          asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(mb) : "memory");
+          asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+          sh.math_abort = 0;
+          sh.panel_abort = 0;
+          sh.ysig[0] = sh.ysig[1] = -1;
+          sh.asig[0] = sh.asig[1] = -1;
+          sh.ycons = -1;
+        }
+      }
+      bar_sync(kBarGang, kAll);
+      const int item = s_item, local = s_local;
+      if (item < 0) break;
+      const PersistParams& p = items[item].p;  // read-only for the whole launch
+      Sync sy(p);
+      const int ntiles = p.TR * p.TC;
+      if (local == ntiles) server_role<BM, BN>(p, sh, sy, threadIdx.x);
+      else if (local == ntiles + 1) yprep_role<BM, BN>(p, sh, sy, threadIdx.x);
+      else math_role<BM, BN>(p, sh, sy, local / p.TC, local % p.TC);
+      bar_sync(kBarGang, kAll);  // the whole CTA is done with the item
+    }
+  } else {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(Cfg<BM, BN>::PanelRegs));
+    for (;;) {
+      bar_sync(kBarGang, kAll);
+      const int item = s_item, local = s_local;
+      if (item < 0) break;
+      const PersistParams& p = items[item].p;
+      Sync sy(p);
+      const int ntiles = p.TR * p.TC;
+      if (local == ntiles) stage_role<BM, BN>(p, sh, sy);
+      else if (local != ntiles + 1) panel_role<BM, BN>(p, sh, sy, local / p.TC, local % p.TC);
+      bar_sync(kBarGang, kAll);
+    }
+  }
+}
+
 }  // namespace
 
 size_t persist_smem_bytes() { return sizeof(Shared); }
+
+cudaError_t launch_persist_gang(const GangItem* items, int count, GangState* state, int grid, long long sched_timeout,
+                                int BM, int BN, cudaStream_t s) {
+  const void* fn = nullptr;
+  if (BM == 96 && BN == 96) fn = (const void*)k_persist_gang<96, 96>;
+  else if (BM == 64 && BN == 64) fn = (const void*)k_persist_gang<64, 64>;
+  else if (BM == 32 && BN == 32) fn = (const void*)k_persist_gang<32, 32>;
+  else return cudaErrorInvalidValue;
+  const size_t smem = sizeof(Shared);
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  void* args[] = {(void*)&items, (void*)&count, (void*)&state, (void*)&sched_timeout};
+  return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(persist_threads(BM, BN)), args, smem, s);
+}
 
 int persist_threads(int BM, int BN) {
   if (BM == 96) return Cfg<96, 96>::Threads;

@@ -61,6 +61,23 @@ inline int persist_flag_words(int TR, int TC) { return TR + 2 * TC + 1 + TR * TC
 constexpr int kPersistExtraCtas = 2;
 inline int persist_cons_words(int TR, int TC) { return 2 * TR + 2 * TC + 2 + 2 * TC + 2 + 2; }
 
+// Several structures in one cooperative launch (gangs of CTAs from a device
+// work queue, see persist.cu).  items are ordered by cost, largest first;
+// ctas = TR * TC + kPersistExtraCtas <= grid.
+struct GangItem {
+  PersistParams p;
+  int ctas;
+  int pad;
+};
+constexpr int kGangMaxCtas = 1024;
+struct GangState {  // zero-initialised before the launch
+  int lock, next, nfree, abort;
+  int pool[kGangMaxCtas];
+  int mail_seq[kGangMaxCtas], mail_item[kGangMaxCtas], mail_local[kGangMaxCtas];
+};
+cudaError_t launch_persist_gang(const GangItem* items, int count, GangState* state, int grid, long long sched_timeout,
+                                int BM, int BN, cudaStream_t s);
+
 size_t persist_smem_bytes();
 int persist_threads(int BM, int BN);
 bool persist_choose_tile(int64_t R, int64_t C, int sms, int* BM, int* BN, bool prefer_large = false);

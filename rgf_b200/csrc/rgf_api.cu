@@ -17,6 +17,7 @@
 #include <atomic>
 #include <string>
 #include <chrono>
+#include <condition_variable>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -42,6 +43,24 @@ struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
 };
+
+struct GangBatch {
+  std::mutex mu;
+  std::condition_variable cv;
+  int pending = 0;  // threads that have neither handed in a sweep nor left
+  bool done = false;
+  cudaError_t result = cudaSuccess;
+  struct Sub {
+    PersistParams p;
+    int ctas;
+    double cost;
+  };
+  std::vector<Sub> subs;
+  int device = 0, sms = 0;
+  cudaStream_t stream = nullptr;
+  int64_t launches = 0;
+};
+
 
 }  // namespace rgf
 
@@ -76,6 +95,9 @@ struct rgf_handle_s {
   // tile tile_bm[i] (first match) when its grid fits the GPU
   std::vector<int64_t> tile_rmax;
   std::vector<int> tile_bm;
+  // batched call in one launch: the coordinator this worker hands its sweep to
+  rgf::GangBatch* gang = nullptr;
+  bool gang_submitted = false;
   int engine_used = 0;     // engine of the last call's final run
   int fallback = 0;        // 1: the persistent engine's result was rejected and recomputed
   double probe_first = 0;  // probe residual of the rejected run
@@ -400,6 +422,93 @@ struct GradReq {
   rgf_cplx* psi = nullptr;
 };
 
+// ---------------------------------------------------------------------------
+// Batched call in one launch.  Every structure of the batch runs the usual
+// pipeline on a host thread of its own (own handle, stream and workspace) up
+// to its persistent sweep; there it hands the sweep's parameters to the
+// coordinator and waits.  When every thread has either handed in its sweep or
+// finished without one, the last to arrive runs all sweeps in ONE cooperative
+// launch of k_persist_gang (gangs of CTAs sized to each structure from a work
+// queue in device memory, largest first), and every thread goes on with its
+// far lead and Fisher-Lee extraction.
+// ---------------------------------------------------------------------------
+// runs the gang launch over every sweep handed in (called by the last thread
+// to arrive, with the lock held)
+void gang_launch(GangBatch* g) {
+  g->done = true;
+  if (g->subs.empty()) return;
+  std::vector<GangBatch::Sub>& v = g->subs;
+  std::stable_sort(v.begin(), v.end(), [](const GangBatch::Sub& a, const GangBatch::Sub& b) { return a.cost > b.cost; });
+  std::vector<GangItem> items(v.size());
+  double est_s = 0.0;
+  for (size_t i = 0; i < v.size(); i++) {
+    items[i].p = v[i].p;
+    items[i].ctas = v[i].ctas;
+    items[i].pad = 0;
+    est_s += v[i].cost;
+  }
+  cudaError_t e = cudaSetDevice(g->device);
+  GangItem* d_items = nullptr;
+  GangState* d_state = nullptr;
+  if (e == cudaSuccess) e = cudaMallocAsync(&d_items, sizeof(GangItem) * items.size(), g->stream);
+  if (e == cudaSuccess) e = cudaMallocAsync(&d_state, sizeof(GangState), g->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_items, items.data(), sizeof(GangItem) * items.size(), cudaMemcpyHostToDevice, g->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_state, 0, sizeof(GangState), g->stream);
+  int clk_khz = 2000000;
+  cudaDeviceGetAttribute(&clk_khz, cudaDevAttrClockRate, g->device);
+  // a free CTA may wait for a whole structure to finish: bound the scheduler's
+  // waits by three times the batch's sequential estimate, at least 30 s
+  const double sched_s = std::max(30.0, 3.0 * est_s);
+  const long long sched_cycles = (long long)(sched_s * 1e3 * clk_khz);
+  if (e == cudaSuccess)
+    e = launch_persist_gang(d_items, (int)items.size(), d_state, g->sms, sched_cycles, 96, 96, g->stream);
+  int abort_word = 0;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&abort_word, &d_state->abort, sizeof(int), cudaMemcpyDeviceToHost, g->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
+  if (d_items) cudaFreeAsync(d_items, g->stream);
+  if (d_state) cudaFreeAsync(d_state, g->stream);
+  cudaStreamSynchronize(g->stream);
+  g->launches++;
+  if (e == cudaSuccess && abort_word) {
+    // the scheduler gave up: no sweep of this launch can be trusted; every
+    // structure raises its own timeout flag so that its call fails
+    for (const GangBatch::Sub& sb : v) {
+      const int bits = kStatusTimeout;
+      cudaMemcpy(sb.p.abort, &bits, sizeof(int), cudaMemcpyHostToDevice);
+      cudaMemcpy(sb.p.status, &bits, sizeof(int), cudaMemcpyHostToDevice);
+    }
+  }
+  if (e != cudaSuccess) cudaGetLastError();
+  g->result = e;
+}
+
+void gang_arrive_locked(GangBatch* g) {
+  if (--g->pending == 0) {
+    gang_launch(g);
+    g->cv.notify_all();
+  }
+}
+
+// a worker's sweep: wait until the gang launch has run it
+cudaError_t gang_run(GangBatch* g, const PersistParams& pp, int BM, int ctas) {
+  std::unique_lock<std::mutex> lock(g->mu);
+  // cost estimate (seconds) for the queue order and the scheduler's bound:
+  // steps x ~25 us per step on 96 x 96 tiles
+  g->subs.push_back({pp, ctas, (double)pp.L * pp.NB * 25e-6});
+  (void)BM;
+  gang_arrive_locked(g);
+  g->cv.wait(lock, [&] { return g->done; });
+  return g->result;
+}
+
+// a worker that finished without handing in a sweep
+void gang_leave(GangBatch* g) {
+  std::lock_guard<std::mutex> lock(g->mu);
+  gang_arrive_locked(g);
+}
+
 // Largest per-slice probe residual max|G_n M_n v - v| (|v_i| = 1) accepted
 // from the persistent engine, whose pivot search stays inside each 32 x 32
 // pivot block: above it (or on a zero / non-finite pivot) the S-matrix is
@@ -643,6 +752,8 @@ rgf_status smatrix_run(rgf_handle h, const Problem& p, const rgf_request* req, c
   };
   int BMp = 0, BNp = 0;
   auto choose_tile = [&]() {
+    // batched call in one launch: the largest tile that fits (fewest SMs per structure)
+    if (h->gang) return persist_choose_tile(Rp, Cp, h->sms, &BMp, &BNp, true);
     for (size_t q = 0; q < h->tile_rmax.size(); q++) {
       if (Rp > h->tile_rmax[q]) continue;
       const int t = h->tile_bm[q];
@@ -748,7 +859,17 @@ rgf_status smatrix_run(rgf_handle h, const Problem& p, const rgf_request* req, c
           std::this_thread::sleep_for(std::chrono::microseconds(20));
         }
       }
-      cudaError_t e = launch_persist(pp, BMp, BNp, h->stream);
+      cudaError_t e;
+      if (h->gang && BMp == 96) {
+        // one launch for the whole batch (96 x 96 tiles): hand the sweep to
+        // the gang launch and wait until it has run; a structure that needs
+        // smaller tiles sweeps on its own before the gang launch
+        RGF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        h->gang_submitted = true;
+        e = gang_run(h->gang, pp, BMp, need);
+      } else {
+        e = launch_persist(pp, BMp, BNp, h->stream);
+      }
       if (h->sm_budget) {
         const cudaError_t se = cudaStreamSynchronize(h->stream);
         h->sm_budget->fetch_add(need);
@@ -757,7 +878,6 @@ rgf_status smatrix_run(rgf_handle h, const Problem& p, const rgf_request* req, c
       if (e != cudaSuccess) {
         cudaGetLastError();
         use_persist = false;  // e.g. the cooperative launch does not fit: per-step engine below
-        probe_d = nullptr;
       } else {
         h->launches++;
         ran_persist = true;
@@ -1265,6 +1385,63 @@ rgf_status rgf_smatrix_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_reques
   return smatrix(h, problem3d(syst), req, opt, S, ldS, ch);
 }
 
+// The batched call in one launch (GangBatch): one host thread and one handle
+// per structure, at most kGangChunk structures per launch.
+constexpr int64_t kGangChunk = 256;
+
+static rgf_status batch_one_launch(rgf_handle h, int64_t count, const rgf_syst2d* systs, const rgf_request* reqs,
+                                   const rgf_options* opt, rgf_cplx* const* S, const int64_t* ldS,
+                                   rgf_status* statuses) {
+  std::vector<rgf_status> res(count, RGF_OK);
+  std::vector<std::string> msg(count);
+  int64_t launches = 0;
+  for (int64_t c0 = 0; c0 < count; c0 += kGangChunk) {
+    const int64_t n = std::min(kGangChunk, count - c0);
+    GangBatch g;
+    g.pending = (int)n;
+    g.device = h->device;
+    g.sms = h->sms;
+    g.stream = h->stream;
+    std::vector<rgf_handle> ws(n, nullptr);
+    std::vector<std::thread> pool;
+    for (int64_t i = 0; i < n; i++) {
+      rgf_status st = rgf_create(h->device, &ws[i]);
+      if (st != RGF_OK) {
+        res[c0 + i] = st;
+        msg[c0 + i] = tl_err;
+        std::lock_guard<std::mutex> lock(g.mu);
+        gang_arrive_locked(&g);
+        continue;
+      }
+      ws[i]->gang = &g;
+      ws[i]->tile_rmax = h->tile_rmax;
+      ws[i]->tile_bm = h->tile_bm;
+      pool.emplace_back([&, i] {
+        rgf_handle w = ws[i];
+        cudaSetDevice(w->device);
+        const int64_t k = c0 + i;
+        res[k] = smatrix(w, problem2d(&systs[k]), &reqs[k], opt, S[k], ldS[k], nullptr);
+        if (res[k] != RGF_OK) msg[k] = tl_err;
+        if (!w->gang_submitted) gang_leave(&g);
+      });
+    }
+    for (auto& th : pool) th.join();
+    launches += g.launches;
+    for (rgf_handle w : ws)
+      if (w) rgf_destroy(w);
+  }
+  h->launches = launches;  // persistent (gang) launches of the call
+  rgf_status first = RGF_OK;
+  for (int64_t i = 0; i < count; i++) {
+    if (statuses) statuses[i] = res[i];
+    if (res[i] != RGF_OK && first == RGF_OK) {
+      first = res[i];
+      set_error("batch item " + std::to_string(i) + ": " + msg[i]);
+    }
+  }
+  return first;
+}
+
 rgf_status rgf_smatrix_batch_2d(rgf_handle h, int64_t count, const rgf_syst2d* systs, const rgf_request* reqs,
                                 const rgf_options* opt, rgf_cplx* const* S, const int64_t* ldS,
                                 rgf_status* statuses, int32_t workers) {
@@ -1279,7 +1456,9 @@ rgf_status rgf_smatrix_batch_2d(rgf_handle h, int64_t count, const rgf_syst2d* s
     set_error("batch: profiling is per call; use rgf_smatrix_2d");
     return RGF_ERR_ARG;
   }
-  int nw = workers > 0 ? workers : 8;
+  RGF_CUDA_TRY(cudaSetDevice(h->device));
+  if (workers <= 0) return batch_one_launch(h, count, systs, reqs, opt, S, ldS, statuses);
+  int nw = workers;
   nw = (int)std::min<int64_t>(nw, count);
   nw = std::max(1, std::min(nw, h->sms / 2));
   RGF_CUDA_TRY(cudaSetDevice(h->device));

@@ -31,7 +31,7 @@ def mixed_batch(n=12, seed=40):
     return systs, outs, ins
 
 
-@pytest.mark.parametrize("workers", [1, 4, 8])
+@pytest.mark.parametrize("workers", [0, 1, 4, 8])
 def test_batch_matches_single_calls(workers):
     systs, outs, ins = mixed_batch()
     Sb = rgf_b200.cal_smatrix_RGF_batch(systs, outs, ins, workers=workers)
@@ -49,10 +49,11 @@ def test_batch_config4_golden():
     cases = [c for c in cases if c is not None]
     if not cases:
         pytest.skip("no config-4 fixtures")
-    Sb = rgf_b200.cal_smatrix_RGF_batch([c["syst"] for c in cases], [c["out"] for c in cases],
-                                        [c["in"] for c in cases], workers=3)
-    for c, S in zip(cases, Sb):
-        assert rel(S, c["S"]) <= TOL_S
+    for workers in (0, 3):  # one launch for all; three pipelines
+        Sb = rgf_b200.cal_smatrix_RGF_batch([c["syst"] for c in cases], [c["out"] for c in cases],
+                                            [c["in"] for c in cases], workers=workers)
+        for c, S in zip(cases, Sb):
+            assert rel(S, c["S"]) <= TOL_S
 
 
 def test_batch_reports_failing_item():
@@ -63,7 +64,21 @@ def test_batch_reports_failing_item():
         bad["epsilon"] = np.ones((9, 3))
     bad["epsilon"][0, 0] = np.nan
     systs[2] = bad
-    with pytest.raises(_abi.RGFError) as ei:
-        rgf_b200.cal_smatrix_RGF_batch(systs, outs, ins, workers=3)
-    assert ei.value.status == _abi.RGF_ERR_NONFINITE
-    assert "batch item 2" in str(ei.value)
+    for workers in (0, 3):
+        with pytest.raises(_abi.RGFError) as ei:
+            rgf_b200.cal_smatrix_RGF_batch(systs, outs, ins, workers=workers)
+        assert ei.value.status == _abi.RGF_ERR_NONFINITE
+        assert "batch item 2" in str(ei.value)
+
+
+def test_one_launch_batch_runs_one_gang_launch():
+    """workers = 0: every sweep of the batch in one persistent launch (gangs
+    from the device work queue), with structures of very different size."""
+    systs, outs, ins = mixed_batch(20, seed=41)
+    h = _abi.Handle(0)
+    Sb = rgf_b200.cal_smatrix_RGF_batch(systs, outs, ins, workers=0, handle=h)
+    launches, _ = h.stats()
+    assert launches == 1
+    for s, o, i, S in zip(systs, outs, ins, Sb):
+        S1, _ = rgf_b200.cal_smatrix_RGF(s, o, i)
+        assert rel(S, S1) <= 1e-12
