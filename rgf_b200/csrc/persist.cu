@@ -1282,11 +1282,11 @@ __global__ void __launch_bounds__(Cfg<BM, BN>::Threads, 1) k_persist(PersistPara
 // out by a work queue in device memory.
 // ---------------------------------------------------------------------------
 // The grid holds one CTA per SM.  A CTA that is free takes the queue's lock,
-// joins the pool of free CTAs and, while the structure at the head of the
-// queue (the items are ordered by cost, largest first) needs no more CTAs
-// than the pool holds, hands it a gang: each gang member gets the item and its
-// place in the item's grid (tile CTA, T-server or prep CTA) through its
-// mailbox.  Every member then runs the role the single-structure kernel would
+// joins the pool of free CTAs and, while one of the first kGangWindow
+// structures not yet dispatched (the items are ordered by cost, largest
+// first) needs no more CTAs than the pool holds, hands the first such one a
+// gang: each gang member gets the item and its place in the item's grid (tile
+// CTA, T-server or prep CTA) through its mailbox.  Every member then runs the role the single-structure kernel would
 // give it, with the item's own exchange buffers and flags; when it returns,
 // the CTA is free again.  Once the queue is empty every CTA in the pool is
 // told to stop.  The head of the queue always fits the grid, so when all
@@ -1331,10 +1331,24 @@ __device__ void gang_next(const GangItem* items, int count, GangState* gs, int m
   int nfree = ldcg_i(&gs->nfree);
   int next = ldcg_i(&gs->next);
   stcg_i(&gs->pool[nfree++], me);
-  while (next < count && items[next].ctas <= nfree) {
-    const int need = items[next].ctas;
-    for (int l = 0; l < need; l++) gang_mail(gs, ldcg_i(&gs->pool[--nfree]), next, l);
-    next++;
+  // dispatch: the first structure within kGangWindow of the head (undispatched
+  // ones, in queue order) that fits the pool, as long as one does; a
+  // dispatched structure is marked taken and the head moves past taken ones
+  for (;;) {
+    int pick = -1;
+    for (int q = next, seen = 0; q < count && seen < kGangWindow; q++) {
+      if (ldcg_i(&gs->taken[q])) continue;
+      seen++;
+      if (items[q].ctas <= nfree) {
+        pick = q;
+        break;
+      }
+    }
+    if (pick < 0) break;
+    stcg_i(&gs->taken[pick], 1);
+    const int need = items[pick].ctas;
+    for (int l = 0; l < need; l++) gang_mail(gs, ldcg_i(&gs->pool[--nfree]), pick, l);
+    while (next < count && ldcg_i(&gs->taken[next])) next++;
   }
   if (next >= count) {
     while (nfree > 0) gang_mail(gs, ldcg_i(&gs->pool[--nfree]), -1, 0);

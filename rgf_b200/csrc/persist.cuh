@@ -70,10 +70,13 @@ struct GangItem {
   int pad;
 };
 constexpr int kGangMaxCtas = 1024;
+constexpr int kGangMaxItems = 256;  // structures per launch
+constexpr int kGangWindow = 8;      // queue positions a free pool may look ahead
 struct GangState {  // zero-initialised before the launch
   int lock, next, nfree, abort;
   int pool[kGangMaxCtas];
   int mail_seq[kGangMaxCtas], mail_item[kGangMaxCtas], mail_local[kGangMaxCtas];
+  int taken[kGangMaxItems];
 };
 cudaError_t launch_persist_gang(const GangItem* items, int count, GangState* state, int grid, long long sched_timeout,
                                 int BM, int BN, cudaStream_t s);

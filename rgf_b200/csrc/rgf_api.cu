@@ -1387,7 +1387,7 @@ rgf_status rgf_smatrix_3d(rgf_handle h, const rgf_syst3d* syst, const rgf_reques
 
 // The batched call in one launch (GangBatch): one host thread and one handle
 // per structure, at most kGangChunk structures per launch.
-constexpr int64_t kGangChunk = 256;
+constexpr int64_t kGangChunk = kGangMaxItems;
 
 static rgf_status batch_one_launch(rgf_handle h, int64_t count, const rgf_syst2d* systs, const rgf_request* reqs,
                                    const rgf_options* opt, rgf_cplx* const* S, const int64_t* ldS,
