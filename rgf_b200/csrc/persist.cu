@@ -1296,6 +1296,12 @@ __global__ void __launch_bounds__(Cfg<BM, BN>::Threads, 1) k_persist(PersistPara
 __device__ __forceinline__ int ldcg_i(const int* p) { return __ldcg(p); }
 __device__ __forceinline__ void stcg_i(int* p, int v) { __stcg(p, v); }
 
+// Parameters of the structures of a gang launch: constant memory, read by
+// every role as the single-structure kernel reads its launch parameters
+// (kept in constant banks, so the roles' register use stays as it is there).
+__constant__ PersistParams c_gang_p[kGangMaxItems];
+static_assert(sizeof(c_gang_p) <= 60 * 1024, "gang parameters must fit the constant bank");
+
 __device__ bool gang_lock(GangState* gs, long long timeout) {
   const long long t0 = clock64();
   while (atomicCAS(&gs->lock, 0, 1) != 0) {
@@ -1323,7 +1329,7 @@ __device__ void gang_mail(GangState* gs, int cta, int item, int local) {
 }
 
 // thread 0 of CTA `me`: the next assignment (item, place), item < 0 = stop
-__device__ void gang_next(const GangItem* items, int count, GangState* gs, int me, int seq, long long timeout,
+__device__ void gang_next(const int* __restrict__ ctas, int count, GangState* gs, int me, int seq, long long timeout,
                           int* item, int* local) {
   *item = -1;
   *local = 0;
@@ -1339,14 +1345,14 @@ __device__ void gang_next(const GangItem* items, int count, GangState* gs, int m
     for (int q = next, seen = 0; q < count && seen < kGangWindow; q++) {
       if (ldcg_i(&gs->taken[q])) continue;
       seen++;
-      if (items[q].ctas <= nfree) {
+      if (ctas[q] <= nfree) {
         pick = q;
         break;
       }
     }
     if (pick < 0) break;
     stcg_i(&gs->taken[pick], 1);
-    const int need = items[pick].ctas;
+    const int need = ctas[pick];
     for (int l = 0; l < need; l++) gang_mail(gs, ldcg_i(&gs->pool[--nfree]), pick, l);
     while (next < count && ldcg_i(&gs->taken[next])) next++;
   }
@@ -1372,7 +1378,7 @@ __device__ void gang_next(const GangItem* items, int count, GangState* gs, int m
 
 template <int BM, int BN>
 __global__ void __launch_bounds__(Cfg<BM, BN>::Threads, 1)
-    k_persist_gang(const GangItem* __restrict__ items, int count, GangState* gs, long long sched_timeout) {
+    k_persist_gang(const int* __restrict__ ctas, int count, GangState* gs, long long sched_timeout) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   Shared& sh = *reinterpret_cast<Shared*>(smem_raw);
   __shared__ int s_item, s_local;
@@ -1386,7 +1392,7 @@ __global__ void __launch_bounds__(Cfg<BM, BN>::Threads, 1)
     for (int seq = 0;; seq++) {
       if (threadIdx.x == 0) {
         int item, local;
-        gang_next(items, count, gs, (int)blockIdx.x, seq, sched_timeout, &item, &local);
+        gang_next(ctas, count, gs, (int)blockIdx.x, seq, sched_timeout, &item, &local);
         s_item = item;
         s_local = local;
         if (item >= 0) {
@@ -1403,7 +1409,7 @@ __global__ void __launch_bounds__(Cfg<BM, BN>::Threads, 1)
       bar_sync(kBarGang, kAll);
       const int item = s_item, local = s_local;
       if (item < 0) break;
-      const PersistParams& p = items[item].p;  // read-only for the whole launch
+      const PersistParams& p = c_gang_p[item];
       Sync sy(p);
       const int ntiles = p.TR * p.TC;
       if (local == ntiles) server_role<BM, BN>(p, sh, sy, threadIdx.x);
@@ -1417,7 +1423,7 @@ __global__ void __launch_bounds__(Cfg<BM, BN>::Threads, 1)
       bar_sync(kBarGang, kAll);
       const int item = s_item, local = s_local;
       if (item < 0) break;
-      const PersistParams& p = items[item].p;
+      const PersistParams& p = c_gang_p[item];
       Sync sy(p);
       const int ntiles = p.TR * p.TC;
       if (local == ntiles) stage_role<BM, BN>(p, sh, sy);
@@ -1431,8 +1437,9 @@ __global__ void __launch_bounds__(Cfg<BM, BN>::Threads, 1)
 
 size_t persist_smem_bytes() { return sizeof(Shared); }
 
-cudaError_t launch_persist_gang(const GangItem* items, int count, GangState* state, int grid, long long sched_timeout,
-                                int BM, int BN, cudaStream_t s) {
+cudaError_t launch_persist_gang(const PersistParams* params, const int* ctas, int count, GangState* state, int grid,
+                                long long sched_timeout, int BM, int BN, cudaStream_t s) {
+  if (count > kGangMaxItems) return cudaErrorInvalidValue;
   const void* fn = nullptr;
   if (BM == 96 && BN == 96) fn = (const void*)k_persist_gang<96, 96>;
   else if (BM == 64 && BN == 64) fn = (const void*)k_persist_gang<64, 64>;
@@ -1441,7 +1448,9 @@ cudaError_t launch_persist_gang(const GangItem* items, int count, GangState* sta
   const size_t smem = sizeof(Shared);
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  void* args[] = {(void*)&items, (void*)&count, (void*)&state, (void*)&sched_timeout};
+  e = cudaMemcpyToSymbolAsync(c_gang_p, params, sizeof(PersistParams) * count, 0, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return e;
+  void* args[] = {(void*)&ctas, (void*)&count, (void*)&state, (void*)&sched_timeout};
   return cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(persist_threads(BM, BN)), args, smem, s);
 }
 

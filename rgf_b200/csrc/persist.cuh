@@ -62,15 +62,12 @@ constexpr int kPersistExtraCtas = 2;
 inline int persist_cons_words(int TR, int TC) { return 2 * TR + 2 * TC + 2 + 2 * TC + 2 + 2; }
 
 // Several structures in one cooperative launch (gangs of CTAs from a device
-// work queue, see persist.cu).  items are ordered by cost, largest first;
-// ctas = TR * TC + kPersistExtraCtas <= grid.
-struct GangItem {
-  PersistParams p;
-  int ctas;
-  int pad;
-};
+// work queue, see persist.cu).  params / ctas (host) are ordered by cost,
+// largest first; ctas[i] = TR * TC + kPersistExtraCtas <= grid; at most
+// kGangMaxItems structures.  Launches that share a device must not overlap
+// (the parameters live in one constant-memory array).
 constexpr int kGangMaxCtas = 1024;
-constexpr int kGangMaxItems = 256;  // structures per launch
+constexpr int kGangMaxItems = 160;  // structures per launch (constant memory)
 constexpr int kGangWindow = 8;      // queue positions a free pool may look ahead
 struct GangState {  // zero-initialised before the launch
   int lock, next, nfree, abort;
@@ -78,8 +75,8 @@ struct GangState {  // zero-initialised before the launch
   int mail_seq[kGangMaxCtas], mail_item[kGangMaxCtas], mail_local[kGangMaxCtas];
   int taken[kGangMaxItems];
 };
-cudaError_t launch_persist_gang(const GangItem* items, int count, GangState* state, int grid, long long sched_timeout,
-                                int BM, int BN, cudaStream_t s);
+cudaError_t launch_persist_gang(const PersistParams* params, const int* ctas, int count, GangState* state, int grid,
+                                long long sched_timeout, int BM, int BN, cudaStream_t s);
 
 size_t persist_smem_bytes();
 int persist_threads(int BM, int BN);

@@ -439,21 +439,25 @@ void gang_launch(GangBatch* g) {
   if (g->subs.empty()) return;
   std::vector<GangBatch::Sub>& v = g->subs;
   std::stable_sort(v.begin(), v.end(), [](const GangBatch::Sub& a, const GangBatch::Sub& b) { return a.cost > b.cost; });
-  std::vector<GangItem> items(v.size());
+  std::vector<PersistParams> params(v.size());
+  std::vector<int> ctas(v.size());
   double est_s = 0.0;
   for (size_t i = 0; i < v.size(); i++) {
-    items[i].p = v[i].p;
-    items[i].ctas = v[i].ctas;
-    items[i].pad = 0;
+    params[i] = v[i].p;
+    ctas[i] = v[i].ctas;
     est_s += v[i].cost;
   }
+  // the launch's parameters live in one constant-memory array per device:
+  // gang launches of the process do not overlap
+  static std::mutex launch_mu;
+  std::lock_guard<std::mutex> launch_lock(launch_mu);
   cudaError_t e = cudaSetDevice(g->device);
-  GangItem* d_items = nullptr;
+  int* d_ctas = nullptr;
   GangState* d_state = nullptr;
-  if (e == cudaSuccess) e = cudaMallocAsync(&d_items, sizeof(GangItem) * items.size(), g->stream);
+  if (e == cudaSuccess) e = cudaMallocAsync(&d_ctas, sizeof(int) * ctas.size(), g->stream);
   if (e == cudaSuccess) e = cudaMallocAsync(&d_state, sizeof(GangState), g->stream);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(d_items, items.data(), sizeof(GangItem) * items.size(), cudaMemcpyHostToDevice, g->stream);
+    e = cudaMemcpyAsync(d_ctas, ctas.data(), sizeof(int) * ctas.size(), cudaMemcpyHostToDevice, g->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(d_state, 0, sizeof(GangState), g->stream);
   int clk_khz = 2000000;
   cudaDeviceGetAttribute(&clk_khz, cudaDevAttrClockRate, g->device);
@@ -462,12 +466,13 @@ void gang_launch(GangBatch* g) {
   const double sched_s = std::max(30.0, 3.0 * est_s);
   const long long sched_cycles = (long long)(sched_s * 1e3 * clk_khz);
   if (e == cudaSuccess)
-    e = launch_persist_gang(d_items, (int)items.size(), d_state, g->sms, sched_cycles, 96, 96, g->stream);
+    e = launch_persist_gang(params.data(), d_ctas, (int)ctas.size(), d_state, g->sms, sched_cycles, 96, 96,
+                            g->stream);
   int abort_word = 0;
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(&abort_word, &d_state->abort, sizeof(int), cudaMemcpyDeviceToHost, g->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(g->stream);
-  if (d_items) cudaFreeAsync(d_items, g->stream);
+  if (d_ctas) cudaFreeAsync(d_ctas, g->stream);
   if (d_state) cudaFreeAsync(d_state, g->stream);
   cudaStreamSynchronize(g->stream);
   g->launches++;
@@ -1021,10 +1026,22 @@ rgf_status smatrix_run(rgf_handle h, const Problem& p, const rgf_request* req, c
       for (int64_t j = k_hi - 1; j >= k_lo; j--) {
         const double2* Wj = segW + (j - k_lo) * Rp * ldm;
         const int nx_ = cur ^ 1;
+        const int64_t n_phys = mirror ? L - 1 - j : j;
+        if (grad_step_fits((int)nI, (int)nO)) {
+          // few channels: both recursions and the contraction in one launch
+          launch_grad_step(Wj, ldm, N, (int)nI, (int)nO, ni_s, no_s, psi[cur], phv[cur], Dd, coef, psi[nx_], phv[nx_],
+                           want_g ? gout + n_phys * N : nullptr, h->stream);
+          h->launches++;
+          if (want_f) {
+            launch_store_field(psi[nx_], idx_d + o_col, N, (int)nI, fout + n_phys * N, N * L, h->stream);
+            h->launches++;
+          }
+          cur = nx_;
+          continue;
+        }
         launch_zgemm_add(N, nI, N, ZOp{Wj, ldm, 0}, ZOp{psi[cur], nI, 0}, ZAdd{Wj + N, ldm, N, ni_s}, psi[nx_],
                          nI, h->stream);
         h->launches++;
-        const int64_t n_phys = mirror ? L - 1 - j : j;
         if (want_f) {
           launch_store_field(psi[nx_], idx_d + o_col, N, (int)nI, fout + n_phys * N, N * L, h->stream);
           h->launches++;

@@ -307,7 +307,8 @@ int sweep_block_width() { return kSw; }
 // of a right-looking LU, so the choices are those of unblocked LU with
 // partial pivoting up to rounding.
 // ---------------------------------------------------------------------------
-constexpr int kGeppThreads = 1024;
+constexpr int kGeppThreads = 512;
+constexpr int kGeppSharedRows = 400;  // panels of up to 400 rows in shared memory (200 KB)
 
 __device__ __forceinline__ void argmax_merge(double& m, int& i, double om, int oi) {
   if (om > m || (om == m && oi >= 0 && (i < 0 || oi < i))) {
@@ -316,13 +317,18 @@ __device__ __forceinline__ void argmax_merge(double& m, int& i, double om, int o
   }
 }
 
+// The panel lives in shared memory when its n x 32 entries fit (n <= 400),
+// in the scratch copy (L2-resident) otherwise.
+template <bool kShared>
 __global__ void __launch_bounds__(kGeppThreads) k_panel_gepp(const double2* __restrict__ M, int64_t ldm,
-                                                             int64_t N, int64_t j0, int jn, double2* __restrict__ P,
+                                                             int64_t N, int64_t j0, int jn, double2* __restrict__ Pg,
                                                              int* __restrict__ swaps, int* status) {
+  extern __shared__ double2 Ps[];
   __shared__ double wmag[kGeppThreads / 32];
   __shared__ int widx[kGeppThreads / 32];
   __shared__ double2 prow[kSw];
   __shared__ int piv_s;
+  double2* P = kShared ? Ps : Pg;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5, nwarps = blockDim.x >> 5;
   const int n = (int)(N - j0);
   for (int64_t e = t; e < (int64_t)n * kSw; e += blockDim.x) {
@@ -361,23 +367,26 @@ __global__ void __launch_bounds__(kGeppThreads) k_panel_gepp(const double2* __re
         piv_s = r;
         swaps[j0 + q] = (int)(j0 + r);
         if (!(best > 0.0) || !isfinite(best)) atomicOr(status, kStatusSingular);
+        // the pivot row (after the exchange) for every thread
       }
     }
     __syncthreads();
     const int r = piv_s;
-    if (r != q && t < kSw) {
-      const double2 a = P[(int64_t)q * kSw + t];
-      P[(int64_t)q * kSw + t] = P[(int64_t)r * kSw + t];
-      P[(int64_t)r * kSw + t] = a;
+    if (t < kSw) {
+      const double2 a = P[(int64_t)q * kSw + t], b = P[(int64_t)r * kSw + t];
+      prow[t] = b;
+      if (r != q) {
+        P[(int64_t)q * kSw + t] = b;
+        P[(int64_t)r * kSw + t] = a;
+      }
     }
-    __syncthreads();
-    if (t < kSw) prow[t] = P[(int64_t)q * kSw + t];
     __syncthreads();
     const double2 d = cinv(prow[q]);
     for (int i = q + 1 + t; i < n; i += blockDim.x) {
-      double2* row = P + (int64_t)i * kSw;
+      double2* __restrict__ row = P + (int64_t)i * kSw;
       const double2 l = cmul(row[q], d);
       row[q] = l;
+#pragma unroll 8
       for (int c = q + 1; c < jn; c++) row[c] = csub(row[c], cmul(l, prow[c]));
     }
     __syncthreads();
@@ -447,7 +456,19 @@ void launch_gepp_step(double2* M, int64_t ldm, int64_t N, int64_t Cc, int64_t j0
                       int* status, cudaStream_t s) {
   double2* P = reinterpret_cast<double2*>(scratch);
   int* swaps = reinterpret_cast<int*>(P + (size_t)N * (kSw + kColpermCtas));
-  k_panel_gepp<<<1, kGeppThreads, 0, s>>>(M, ldm, N, j0, jn, P, swaps, status);
+  const int64_t n = N - j0;
+  const size_t sm = sizeof(double2) * (size_t)n * kSw;
+  if (n <= kGeppSharedRows) {
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(k_panel_gepp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)(sizeof(double2) * kGeppSharedRows * kSw));
+      attr = true;
+    }
+    k_panel_gepp<true><<<1, kGeppThreads, sm, s>>>(M, ldm, N, j0, jn, P, swaps, status);
+  } else {
+    k_panel_gepp<false><<<1, kGeppThreads, 0, s>>>(M, ldm, N, j0, jn, P, swaps, status);
+  }
   k_laswp<<<(unsigned)((Cc + 255) / 256), 256, 0, s>>>(M, ldm, Cc, j0, jn, swaps);
 }
 
@@ -719,6 +740,115 @@ void launch_grad_fused(const double2* Phi, const double2* Psi, const double2* D,
                        double2 coef, double2* g, cudaStream_t s) {
   k_grad_fused<<<(unsigned)((N + 127) / 128), 128, sizeof(double2) * n_out * n_in, s>>>(Phi, Psi, D, N, n_out,
                                                                                         n_in, coef, g);
+}
+
+// One slice of the backward recursions and the gradient contraction in one
+// launch, for few channels (n_in, n_out <= kGradFusedMax):
+//   Psi_out = g_j Psi_in + [X_j, 0]      (N x n_in)
+//   Phi_out = Phi_in g_j + [Z_j; 0]      (n_out x N)
+//   g[m]    = coef sum_a Phi_out[a][m] sum_b D[a][b] Psi_out[m][b]
+// with g_j = W(0:N, 0:N), X_j = W(0:N, N:N+ni_s), Z_j = W(N:N+no_s, 0:N)
+// (W row-major, leading dimension ld).  CTA c owns sites [16c, 16c+16):
+// those rows of Psi_out and columns of Phi_out, accumulated over K in chunks
+// of 16 staged in shared memory, then their contraction.
+constexpr int kGradFusedMax = 32;
+constexpr int kGTM = 16, kGKC = 16;
+
+__global__ void __launch_bounds__(256) k_grad_step(const double2* __restrict__ W, int64_t ld, int64_t N, int n_in,
+                                                   int n_out, int ni_s, int no_s, const double2* __restrict__ Psi_in,
+                                                   const double2* __restrict__ Phi_in, const double2* __restrict__ D,
+                                                   double2 coef, double2* __restrict__ Psi_out,
+                                                   double2* __restrict__ Phi_out, double2* __restrict__ g) {
+  __shared__ double2 sPsi[kGKC][kGradFusedMax];   // Psi_in chunk (k, b)
+  __shared__ double2 sPhi[kGradFusedMax][kGKC];   // Phi_in chunk (a, k)
+  __shared__ double2 sWr[kGTM][kGKC + 1];         // W rows of my sites, chunk columns
+  __shared__ double2 sWc[kGKC][kGTM + 1];         // W chunk rows, columns of my sites
+  __shared__ double2 oPsi[kGTM][kGradFusedMax];   // results of my sites
+  __shared__ double2 oPhi[kGradFusedMax][kGTM];
+  const int t = threadIdx.x;
+  const int64_t m0 = (int64_t)blockIdx.x * kGTM;
+  const int tm = (int)min((int64_t)kGTM, N - m0);
+  // each thread: up to two Psi outputs (m, b) and two Phi outputs (a, m)
+  double2 accP[2] = {cmk(0, 0), cmk(0, 0)}, accF[2] = {cmk(0, 0), cmk(0, 0)};
+  for (int64_t k0 = 0; k0 < N; k0 += kGKC) {
+    const int kc = (int)min((int64_t)kGKC, N - k0);
+    for (int e = t; e < kGKC * kGradFusedMax; e += 256) {
+      const int k = e / kGradFusedMax, b = e % kGradFusedMax;
+      sPsi[k][b] = (k < kc && b < n_in) ? Psi_in[(k0 + k) * n_in + b] : cmk(0, 0);
+    }
+    for (int e = t; e < kGradFusedMax * kGKC; e += 256) {
+      const int a = e / kGKC, k = e % kGKC;
+      sPhi[a][k] = (k < kc && a < n_out) ? Phi_in[(int64_t)a * N + k0 + k] : cmk(0, 0);
+    }
+    for (int e = t; e < kGTM * kGKC; e += 256) {
+      const int r = e / kGKC, k = e % kGKC;
+      sWr[r][k] = (r < tm && k < kc) ? W[(m0 + r) * ld + k0 + k] : cmk(0, 0);
+    }
+    for (int e = t; e < kGKC * kGTM; e += 256) {
+      const int k = e / kGTM, c = e % kGTM;
+      sWc[k][c] = (k < kc && c < tm) ? W[(k0 + k) * ld + m0 + c] : cmk(0, 0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int o = t + 256 * q;  // Psi output o = r * 32 + b; Phi output o = a * 16 + c
+      const int r = o / kGradFusedMax, b = o % kGradFusedMax;
+      const int a = o / kGTM, c = o % kGTM;
+      double2 sp = accP[q], sf = accF[q];
+      for (int k = 0; k < kc; k++) {
+        sp = cadd(sp, cmul(sWr[r][k], sPsi[k][b]));
+        sf = cadd(sf, cmul(sPhi[a][k], sWc[k][c]));
+      }
+      accP[q] = sp;
+      accF[q] = sf;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    const int o = t + 256 * q;
+    const int r = o / kGradFusedMax, b = o % kGradFusedMax;
+    const int a = o / kGTM, c = o % kGTM;
+    if (r < tm && b < n_in) {
+      double2 v = accP[q];
+      if (b < ni_s) v = cadd(v, W[(m0 + r) * ld + N + b]);
+      Psi_out[(m0 + r) * n_in + b] = v;
+      oPsi[r][b] = v;
+    }
+    if (c < tm && a < n_out) {
+      double2 v = accF[q];
+      if (a < no_s) v = cadd(v, W[(N + a) * ld + m0 + c]);
+      Phi_out[(int64_t)a * N + m0 + c] = v;
+      oPhi[a][c] = v;
+    }
+  }
+  if (!g) return;
+  __syncthreads();
+  // g[m] = coef sum_a Phi[a][m] (D Psi^T)[a][m]: warp w handles site w, w+8
+  const int lane = t & 31, warp = t >> 5;
+  for (int r = warp; r < tm; r += 8) {
+    double2 acc = cmk(0, 0);
+    for (int a = lane; a < n_out; a += 32) {
+      double2 e = cmk(0, 0);
+      for (int b = 0; b < n_in; b++) e = cadd(e, cmul(D[a * n_in + b], oPsi[r][b]));
+      acc = cadd(acc, cmul(oPhi[a][r], e));
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
+      acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
+    }
+    if (lane == 0) g[m0 + r] = cmul(coef, acc);
+  }
+}
+
+bool grad_step_fits(int n_in, int n_out) { return n_in <= kGradFusedMax && n_out <= kGradFusedMax; }
+
+void launch_grad_step(const double2* W, int64_t ld, int64_t N, int n_in, int n_out, int ni_s, int no_s,
+                      const double2* Psi_in, const double2* Phi_in, const double2* D, double2 coef, double2* Psi_out,
+                      double2* Phi_out, double2* g, cudaStream_t s) {
+  k_grad_step<<<(unsigned)((N + kGTM - 1) / kGTM), 256, 0, s>>>(W, ld, N, n_in, n_out, ni_s, no_s, Psi_in, Phi_in, D,
+                                                                coef, Psi_out, Phi_out, g);
 }
 
 // g[m] = coef * sum_a Phi[a][m] Et[a][m]  (Phi, Et: n_out x N row-major)

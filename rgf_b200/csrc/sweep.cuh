@@ -64,6 +64,12 @@ void launch_add_identity(double2* M, int64_t ldm, int64_t n, cudaStream_t s);
 // fields: out[m + i*ld] = Psi[m][col_of[i]]
 void launch_store_field(const double2* Psi, const int* col_of, int64_t N, int n_in, double2* out, int64_t ld,
                         cudaStream_t s);
+// one slice of the backward recursions (and the contraction when g) in one
+// launch, for n_in, n_out <= 32 (grad_step_fits)
+bool grad_step_fits(int n_in, int n_out);
+void launch_grad_step(const double2* W, int64_t ld, int64_t N, int n_in, int n_out, int ni_s, int no_s,
+                      const double2* Psi_in, const double2* Phi_in, const double2* D, double2 coef, double2* Psi_out,
+                      double2* Phi_out, double2* g, cudaStream_t s);
 void launch_grad_slice(const double2* Phi, const double2* Et, int64_t N, int64_t n_out, double2 coef, double2* g,
                        cudaStream_t s);
 

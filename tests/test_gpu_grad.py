@@ -169,3 +169,18 @@ def test_torch_autograd_harness():
     S_np = S.detach().numpy()
     _, g = rgf_b200.smatrix_grad_RGF(dict(syst, epsilon=eps.detach().numpy()), out, inp, np.conj(S_np))
     assert np.abs(eps.grad.numpy() - 2 * np.real(g)).max() <= 1e-12 * np.abs(2 * np.real(g)).max()
+
+
+def test_gradient_many_channels():
+    """More than 32 channels on a side: the backward pass takes its GEMM path
+    (the one-launch step serves up to 32 x 32)."""
+    rng = np.random.default_rng(30)
+    syst = dict(epsilon=1 + 2 * rng.random((260, 4)), epsilon_L=1.0, epsilon_R=1.0, k0dx=2 * np.pi / 15,
+                yBC="periodic")
+    out, inp = ["left", "right"], ["left", "right"]
+    S0, _ = ref_smatrix(syst, out, inp)
+    assert min(S0.shape) > 64
+    D = np.conj(S0)
+    _, g = rgf_b200.smatrix_grad_RGF(syst, out, inp, D, checkpoint=2)
+    _, g0 = grad_rgf_2d(syst, out, inp, D)
+    assert relmax(g, g0) <= TOL_G
