@@ -272,11 +272,13 @@ def grad_over_fwd(h, dev, stream, reps: int = 5):
                         "F = sum|t|^2, checkpoint every 23 slices"}
 
 
-def batch_rate(dev, count: int = 256, workers: int = 16):
+def batch_rate(dev, count: int = 256, workers: int = 0):
     """Config-4 batched form: all 256 seeded structures (N uniform 64..512,
     L uniform 100..2000, eps 1+2U, complex k0dx), full S each, through
-    rgf_smatrix_batch_2d with host inputs and outputs; timed by the host
-    around the blocking call (warm-up call on four structures first)."""
+    rgf_smatrix_batch_2d with host inputs and outputs (workers = 0: every
+    sweep in one persistent launch per 160 structures; > 0: that many
+    concurrent pipelines); timed by the host around the blocking call
+    (warm-up call on four structures first)."""
     import rgf_b200
     from rgf_b200 import workloads
     items = [workloads.config4_structure(k) for k in range(count)]
@@ -290,7 +292,7 @@ def batch_rate(dev, count: int = 256, workers: int = 16):
     Ns, Ls, _ = workloads.config4_params()
     return {"value": count / dt, "unit": "S-matrices/s", "structures": count, "workers": workers,
             "seconds": dt, "sum_L_N3": float(np.sum(Ls[:count].astype(float) * Ns[:count].astype(float) ** 3)),
-            "workload": "config4: first structures of the 256-structure batch (N U{64..512}, L U{100..2000}, "
+            "workload": "config4: the 256-structure batch (N U{64..512}, L U{100..2000}, "
                         "eps 1+2U, k0dx = 2pi/15 (1 + i eta), eta U[0,1e-3), periodic, full S)",
             "timing": "host wall clock around the blocking batch call; inputs and S on the host"}
 
@@ -397,7 +399,8 @@ def run_ours(args, dist):
     line["canonical_tflops"] = F * value / 1e12 / dist.world
     line["precision_form"] = None
     line["grad_over_fwd"] = grad_over_fwd(h, dev, stream) if not args.slices else None
-    line["batch"] = batch_rate(dev) if not args.slices else None
+    line["batch"] = batch_rate(dev, workers=0) if not args.slices else None
+    line["batch_pipelines"] = batch_rate(dev, workers=16) if not args.slices else None
     n, ms, fl_exec, name = prof
     fl = nx * workloads.canonical_slice_flops(ny, n_in // 2, n_out // 2)  # the launch covers all nx slices
     achieved = fl / (ms / n / 1e3) / 1e12 if n else None

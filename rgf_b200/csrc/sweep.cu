@@ -750,88 +750,99 @@ void launch_grad_fused(const double2* Phi, const double2* Psi, const double2* D,
 // with g_j = W(0:N, 0:N), X_j = W(0:N, N:N+ni_s), Z_j = W(N:N+no_s, 0:N)
 // (W row-major, leading dimension ld).  CTA c owns sites [16c, 16c+16):
 // those rows of Psi_out and columns of Phi_out, accumulated over K in chunks
-// of 16 staged in shared memory, then their contraction.
+// of up to 128 staged in (dynamic) shared memory, then their contraction.
 constexpr int kGradFusedMax = 32;
-constexpr int kGTM = 16, kGKC = 16;
+constexpr int kGTM = 16, kGKC = 128;
+
+__host__ __device__ inline size_t grad_step_smem(int n_in, int n_out) {
+  // sPsi[KC][n_in], sPhi[n_out][KC], sWr[16][KC+1], sWc[KC][17], oPsi[16][n_in], oPhi[n_out][16]
+  return sizeof(double2) * ((size_t)kGKC * n_in + (size_t)n_out * kGKC + kGTM * (kGKC + 1) + kGKC * (kGTM + 1) +
+                            kGTM * n_in + (size_t)n_out * kGTM);
+}
 
 __global__ void __launch_bounds__(256) k_grad_step(const double2* __restrict__ W, int64_t ld, int64_t N, int n_in,
                                                    int n_out, int ni_s, int no_s, const double2* __restrict__ Psi_in,
                                                    const double2* __restrict__ Phi_in, const double2* __restrict__ D,
                                                    double2 coef, double2* __restrict__ Psi_out,
                                                    double2* __restrict__ Phi_out, double2* __restrict__ g) {
-  __shared__ double2 sPsi[kGKC][kGradFusedMax];   // Psi_in chunk (k, b)
-  __shared__ double2 sPhi[kGradFusedMax][kGKC];   // Phi_in chunk (a, k)
-  __shared__ double2 sWr[kGTM][kGKC + 1];         // W rows of my sites, chunk columns
-  __shared__ double2 sWc[kGKC][kGTM + 1];         // W chunk rows, columns of my sites
-  __shared__ double2 oPsi[kGTM][kGradFusedMax];   // results of my sites
-  __shared__ double2 oPhi[kGradFusedMax][kGTM];
+  extern __shared__ double2 gsm[];
+  double2* sPsi = gsm;                               // [KC][n_in]
+  double2* sPhi = sPsi + kGKC * n_in;                // [n_out][KC]
+  double2* sWr = sPhi + n_out * kGKC;                // [16][KC + 1]
+  double2* sWc = sWr + kGTM * (kGKC + 1);            // [KC][17]
+  double2* oPsi = sWc + kGKC * (kGTM + 1);           // [16][n_in]
+  double2* oPhi = oPsi + kGTM * n_in;                // [n_out][16]
   const int t = threadIdx.x;
   const int64_t m0 = (int64_t)blockIdx.x * kGTM;
   const int tm = (int)min((int64_t)kGTM, N - m0);
-  // each thread: up to two Psi outputs (m, b) and two Phi outputs (a, m)
+  const int nP = kGTM * n_in, nF = n_out * kGTM;  // outputs of this CTA (<= 512 each)
   double2 accP[2] = {cmk(0, 0), cmk(0, 0)}, accF[2] = {cmk(0, 0), cmk(0, 0)};
   for (int64_t k0 = 0; k0 < N; k0 += kGKC) {
     const int kc = (int)min((int64_t)kGKC, N - k0);
-    for (int e = t; e < kGKC * kGradFusedMax; e += 256) {
-      const int k = e / kGradFusedMax, b = e % kGradFusedMax;
-      sPsi[k][b] = (k < kc && b < n_in) ? Psi_in[(k0 + k) * n_in + b] : cmk(0, 0);
+    for (int e = t; e < kc * n_in; e += 256) sPsi[e] = Psi_in[k0 * n_in + e];  // rows k0.. of Psi_in, contiguous
+    for (int e = t; e < n_out * kc; e += 256) {
+      const int a = e / kc, k = e % kc;
+      sPhi[a * kGKC + k] = Phi_in[(int64_t)a * N + k0 + k];
     }
-    for (int e = t; e < kGradFusedMax * kGKC; e += 256) {
-      const int a = e / kGKC, k = e % kGKC;
-      sPhi[a][k] = (k < kc && a < n_out) ? Phi_in[(int64_t)a * N + k0 + k] : cmk(0, 0);
+    for (int e = t; e < kGTM * kc; e += 256) {
+      const int r = e / kc, k = e % kc;
+      sWr[r * (kGKC + 1) + k] = (r < tm) ? W[(m0 + r) * ld + k0 + k] : cmk(0, 0);
     }
-    for (int e = t; e < kGTM * kGKC; e += 256) {
-      const int r = e / kGKC, k = e % kGKC;
-      sWr[r][k] = (r < tm && k < kc) ? W[(m0 + r) * ld + k0 + k] : cmk(0, 0);
-    }
-    for (int e = t; e < kGKC * kGTM; e += 256) {
+    for (int e = t; e < kc * kGTM; e += 256) {
       const int k = e / kGTM, c = e % kGTM;
-      sWc[k][c] = (k < kc && c < tm) ? W[(k0 + k) * ld + m0 + c] : cmk(0, 0);
+      sWc[k * (kGTM + 1) + c] = (c < tm) ? W[(k0 + k) * ld + m0 + c] : cmk(0, 0);
     }
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < 2; q++) {
-      const int o = t + 256 * q;  // Psi output o = r * 32 + b; Phi output o = a * 16 + c
-      const int r = o / kGradFusedMax, b = o % kGradFusedMax;
-      const int a = o / kGTM, c = o % kGTM;
-      double2 sp = accP[q], sf = accF[q];
-      for (int k = 0; k < kc; k++) {
-        sp = cadd(sp, cmul(sWr[r][k], sPsi[k][b]));
-        sf = cadd(sf, cmul(sPhi[a][k], sWc[k][c]));
+      const int o = t + 256 * q;
+      if (o < nP) {
+        const int r = o / n_in, b = o % n_in;
+        double2 sp = accP[q];
+        for (int k = 0; k < kc; k++) sp = cadd(sp, cmul(sWr[r * (kGKC + 1) + k], sPsi[k * n_in + b]));
+        accP[q] = sp;
       }
-      accP[q] = sp;
-      accF[q] = sf;
+      if (o < nF) {
+        const int a = o / kGTM, c = o % kGTM;
+        double2 sf = accF[q];
+        for (int k = 0; k < kc; k++) sf = cadd(sf, cmul(sPhi[a * kGKC + k], sWc[k * (kGTM + 1) + c]));
+        accF[q] = sf;
+      }
     }
     __syncthreads();
   }
 #pragma unroll
   for (int q = 0; q < 2; q++) {
     const int o = t + 256 * q;
-    const int r = o / kGradFusedMax, b = o % kGradFusedMax;
-    const int a = o / kGTM, c = o % kGTM;
-    if (r < tm && b < n_in) {
-      double2 v = accP[q];
-      if (b < ni_s) v = cadd(v, W[(m0 + r) * ld + N + b]);
-      Psi_out[(m0 + r) * n_in + b] = v;
-      oPsi[r][b] = v;
+    if (o < nP) {
+      const int r = o / n_in, b = o % n_in;
+      if (r < tm) {
+        double2 v = accP[q];
+        if (b < ni_s) v = cadd(v, W[(m0 + r) * ld + N + b]);
+        Psi_out[(m0 + r) * n_in + b] = v;
+        oPsi[r * n_in + b] = v;
+      }
     }
-    if (c < tm && a < n_out) {
-      double2 v = accF[q];
-      if (a < no_s) v = cadd(v, W[(N + a) * ld + m0 + c]);
-      Phi_out[(int64_t)a * N + m0 + c] = v;
-      oPhi[a][c] = v;
+    if (o < nF) {
+      const int a = o / kGTM, c = o % kGTM;
+      if (c < tm) {
+        double2 v = accF[q];
+        if (a < no_s) v = cadd(v, W[(N + a) * ld + m0 + c]);
+        Phi_out[(int64_t)a * N + m0 + c] = v;
+        oPhi[a * kGTM + c] = v;
+      }
     }
   }
   if (!g) return;
   __syncthreads();
-  // g[m] = coef sum_a Phi[a][m] (D Psi^T)[a][m]: warp w handles site w, w+8
+  // g[m] = coef sum_a Phi[a][m] (D Psi^T)[a][m]: warp w handles sites w, w + 8
   const int lane = t & 31, warp = t >> 5;
   for (int r = warp; r < tm; r += 8) {
     double2 acc = cmk(0, 0);
     for (int a = lane; a < n_out; a += 32) {
       double2 e = cmk(0, 0);
-      for (int b = 0; b < n_in; b++) e = cadd(e, cmul(D[a * n_in + b], oPsi[r][b]));
-      acc = cadd(acc, cmul(oPhi[a][r], e));
+      for (int b = 0; b < n_in; b++) e = cadd(e, cmul(D[a * n_in + b], oPsi[r * n_in + b]));
+      acc = cadd(acc, cmul(oPhi[a * kGTM + r], e));
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
@@ -847,8 +858,14 @@ bool grad_step_fits(int n_in, int n_out) { return n_in <= kGradFusedMax && n_out
 void launch_grad_step(const double2* W, int64_t ld, int64_t N, int n_in, int n_out, int ni_s, int no_s,
                       const double2* Psi_in, const double2* Phi_in, const double2* D, double2 coef, double2* Psi_out,
                       double2* Phi_out, double2* g, cudaStream_t s) {
-  k_grad_step<<<(unsigned)((N + kGTM - 1) / kGTM), 256, 0, s>>>(W, ld, N, n_in, n_out, ni_s, no_s, Psi_in, Phi_in, D,
-                                                                coef, Psi_out, Phi_out, g);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_grad_step, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)grad_step_smem(kGradFusedMax, kGradFusedMax));
+    attr = true;
+  }
+  k_grad_step<<<(unsigned)((N + kGTM - 1) / kGTM), 256, grad_step_smem(n_in, n_out), s>>>(
+      W, ld, N, n_in, n_out, ni_s, no_s, Psi_in, Phi_in, D, coef, Psi_out, Phi_out, g);
 }
 
 // g[m] = coef * sum_a Phi[a][m] Et[a][m]  (Phi, Et: n_out x N row-major)
