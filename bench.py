@@ -47,7 +47,7 @@ UNIT = "S-matrices/s"
 FP64_DMMA_FALLBACK_TFLOPS = 37.0  # earlier measurement on this pool, used only if the live one fails
 PROFILE_EVERY = 64
 REF_ARM_SLICES = 32  # slices the reference arm samples per timed step
-DRAM_BYTES_PER_SLICE = (20.995072e6 + 8.149248e6) / 16  # k_persist<96,96>, config 2, ncu over 16 slices
+DRAM_BYTES_PER_SLICE = (21.144832e6 + 12.653056e6) / 16  # k_persist<96,96>, config 2, ncu over 16 slices
 
 
 def log(*a):
