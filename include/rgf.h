@@ -164,7 +164,7 @@ RGF_API rgf_status rgf_smatrix_3d(rgf_handle h, const rgf_syst3d* syst, const rg
  * set-up runs on a host thread and stream of its own, and all their slice
  * sweeps run in ONE persistent cooperative launch in which gangs of CTAs,
  * sized to each structure, take the structures from a work queue in device
- * memory, largest first (at most 256 structures per launch; a structure that
+ * memory, largest first (at most 160 structures per launch; a structure that
  * needs tiles smaller than 96 x 96 sweeps on its own first).  workers > 0:
  * that many concurrent pipelines (host threads, each with its own stream and
  * workspace), whose persistent sweeps share the GPU's SMs through one budget.
