@@ -1283,8 +1283,8 @@ __global__ void __launch_bounds__(Cfg<BM, BN>::Threads, 1) k_persist(PersistPara
 // ---------------------------------------------------------------------------
 // The grid holds one CTA per SM.  A CTA that is free takes the queue's lock,
 // joins the pool of free CTAs and, while a structure not yet dispatched fits
-// the pool (the items are ordered by cost, largest first: the head if it
-// fits, else the smallest that does), hands it a gang: each gang member gets
+// the pool (the items are ordered by cost, largest first: the first that
+// fits among the kGangWindow next ones), hands it a gang: each gang member gets
 // the item and its place in the item's grid (tile CTA, T-server or prep CTA)
 // through its mailbox.  Every member then runs the role the single-structure kernel would
 // give it, with the item's own exchange buffers and flags; when it returns,
@@ -1337,22 +1337,19 @@ __device__ void gang_next(const int* __restrict__ ctas, int count, GangState* gs
   int nfree = ldcg_i(&gs->nfree);
   int next = ldcg_i(&gs->next);
   stcg_i(&gs->pool[nfree++], me);
-  // dispatch, as long as something fits the pool: the head of the queue (the
-  // largest structure not yet dispatched) if it fits, else the smallest that
-  // does (scanning from the tail), so that CTAs the head cannot use yet do
-  // not idle; the head gets the pool as soon as enough CTAs are free again.
-  // A dispatched structure is marked taken; the head moves past taken ones.
+  // dispatch, as long as something fits the pool: the first structure, in
+  // queue order, among the kGangWindow next ones not yet dispatched that fits
+  // (the head whenever it fits; smaller ones behind it fill CTAs the head
+  // cannot use yet).  A dispatched structure is marked taken; the head moves
+  // past taken ones.
   for (;;) {
     int pick = -1;
-    if (next < count && ctas[next] <= nfree) {
-      pick = next;
-    } else {
-      for (int q = count - 1; q > next; q--) {
-        if (ldcg_i(&gs->taken[q])) continue;
-        if (ctas[q] <= nfree) {
-          pick = q;
-          break;
-        }
+    for (int q = next, seen = 0; q < count && seen < kGangWindow; q++) {
+      if (ldcg_i(&gs->taken[q])) continue;
+      seen++;
+      if (ctas[q] <= nfree) {
+        pick = q;
+        break;
       }
     }
     if (pick < 0) break;

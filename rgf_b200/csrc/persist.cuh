@@ -68,6 +68,7 @@ inline int persist_cons_words(int TR, int TC) { return 2 * TR + 2 * TC + 2 + 2 *
 // (the parameters live in one constant-memory array).
 constexpr int kGangMaxCtas = 1024;
 constexpr int kGangMaxItems = 160;  // structures per launch (constant memory)
+constexpr int kGangWindow = 16;     // queue positions a free pool may look ahead
 struct GangState {  // zero-initialised before the launch
   int lock, next, nfree, abort;
   int pool[kGangMaxCtas];
