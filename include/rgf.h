@@ -116,11 +116,9 @@ typedef struct {
 typedef struct {
   int32_t precision;  /* rgf_precision (0 = RGF_FP64)                                  */
   int32_t engine;     /* 0 (default): persistent register-resident sweep kernel when
-                         the matrix fits on the GPU, with diagonal pivots (each
-                         checked against its column), then, if a check fails,
-                         with pivoting inside each 32 x 32 pivot block; every
-                         slice inverse is checked a posteriori and the call is
-                         recomputed with engine 1 if one still fails.
+                         the matrix fits on the GPU, pivoting inside each 32 x 32
+                         pivot block; every slice inverse is checked a posteriori
+                         and the call is recomputed with engine 1 if one fails.
                          1: one launch sequence per pivot step with partial
                          pivoting over the whole column (LAPACK zgetrf's choice,
                          as MATLAB's inv)                                            */
@@ -268,14 +266,10 @@ RGF_API const char* rgf_version(void);
  * the swept matrix). */
 RGF_API rgf_status rgf_last_stats(rgf_handle h, int64_t* kernel_launches, double* probe_residual);
 /* Engine that produced the last rgf_smatrix_* result on this handle (0 or 1,
- * see rgf_options.engine) and how many times the call was recomputed: the
- * persistent engine first takes the diagonal entries as pivots (each checked
- * against a tenth of its column's largest magnitude); a failed check (such a
- * weak pivot, a zero or non-finite pivot, a probe residual above 1e-10)
- * recomputes with partial pivoting inside each 32 x 32 block (fallback = 1),
- * and a second failure with engine 1 (fallback = 2, or 1 when the first run
- * already pivoted).  rejected_probe is the first run's residual.  An addition
- * of this library. */
+ * see rgf_options.engine); fallback = 1 when the persistent engine's result
+ * was rejected by the a-posteriori check (a zero or non-finite in-block
+ * pivot, or a probe residual above 1e-10) and recomputed with engine 1;
+ * rejected_probe is that run's residual.  An addition of this library. */
 RGF_API rgf_status rgf_last_engine(rgf_handle h, int32_t* engine, int32_t* fallback, double* rejected_probe);
 /* Sampled timing of the dominant kernel of the last rgf_smatrix_* call made
  * with opt->profile > 0: number of timed launches, their summed duration (ms),

@@ -152,7 +152,6 @@ struct Shared {
   int gflag[kPB];
   double2 drow[kPB];
   int gj_fail;  // a Gauss-Jordan wait gave up
-  int gj_weak;  // a diagonal pivot was below a tenth of its column's largest entry
   int asig[2];  // T-server: step whose a3[parity] block is staged (prep -> server)
   int ysig[2];  // T-server: step whose y[parity] blocks are ready (prep -> server)
   int ycons;    // T-server: last step whose y blocks the server has read
@@ -913,12 +912,7 @@ __device__ void panel_role(const PersistParams& p, Shared& sh, const Sync& sy, i
 // single-precision magnitudes packed with the lane index, the reciprocal
 // formed speculatively by every lane meanwhile.  Row interchanges are
 // implicit:  inv[pinv[r]][perm[c]] = a(r, c),  perm[q] = row chosen at q.
-// Without kPivot the pivots are the diagonal entries, in order (no search on
-// the chain); the same reduction, off the chain, only checks that each is at
-// least a tenth of its column's largest magnitude (else sh.gj_weak is set and
-// the call is recomputed with pivoting).
 // Returns false in every lane if a wait gave up (abort or timeout).
-template <bool kPivot>
 __device__ __forceinline__ bool gj_ahead(const PersistParams& p, Shared& sh, double2 (&a)[4], int t) {
   constexpr int NC = 4;
   const int lane = t & 31, warp = t >> 5;
@@ -930,28 +924,18 @@ __device__ __forceinline__ bool gj_ahead(const PersistParams& p, Shared& sh, dou
       for (int cq = 0; cq < NC; cq++) {
         const int q = b * NC + cq;
         const double2 vq = a[cq];
-        const double2 dq = crecip_nr(vq);  // speculative: used only if this lane is the pivot
+        const double2 dq = crecip_nr(vq);  // speculative: used only if this lane wins
         const float fx = (float)vq.x, fy = (float)vq.y;
         const float mag = fx * fx + fy * fy;
         const bool elig = !((used >> lane) & 1u);
         const unsigned key = elig ? ((__float_as_uint(mag) & ~63u) | (unsigned)(32 - lane)) : 0u;
         const unsigned best = __reduce_max_sync(kFull, key);
-        int pv;
-        if (kPivot) {
-          pv = 32 - (int)(best & 63u);
-        } else {
-          // diagonal pivot; the column maximum only checks it (off the chain):
-          // a pivot below a tenth of the column's largest magnitude is weak
-          pv = q;
-          const float dmag = __shfl_sync(kFull, mag, q);
-          const float bmag = __uint_as_float(best & ~63u);
-          if (lane == 0 && !(dmag >= 0.01f * bmag)) sh.gj_weak = 1;
-        }
+        const int pv = 32 - (int)(best & 63u);
         const double2 d = cmk(__shfl_sync(kFull, dq.x, pv), __shfl_sync(kFull, dq.y, pv));
         const bool me = lane == pv;
         const double2 m = me ? cmk(0.0, 0.0) : cmul(vq, d);
         sh.srv.v[q][lane] = m;
-        if (kPivot) sh.gpiv[q][lane] = pv;
+        sh.gpiv[q][lane] = pv;
         if (me) {
           sh.drow[lane] = d;
           sh.pinv[lane] = q;
@@ -960,8 +944,7 @@ __device__ __forceinline__ bool gj_ahead(const PersistParams& p, Shared& sh, dou
         st_release_cta(&sh.gflag[lane], q + 1);
         // a zero reciprocal of a nonzero pivot (|z|^2 beyond the range of
         // rcp.approx.ftz) is as unusable as a non-finite one
-        sing = sing || (kPivot && (best >> 6) == 0u) || !isfinite(d.x) || !isfinite(d.y) ||
-               (d.x == 0.0 && d.y == 0.0);
+        sing = sing || (best >> 6) == 0u || !isfinite(d.x) || !isfinite(d.y) || (d.x == 0.0 && d.y == 0.0);
         used |= 1u << pv;
 #pragma unroll
         for (int c = 0; c < NC; c++) {
@@ -988,7 +971,7 @@ __device__ __forceinline__ bool gj_ahead(const PersistParams& p, Shared& sh, dou
           }
         }
         const double2 m = sh.srv.v[q][lane];
-        const int pv = kPivot ? (sh.gpiv[q][lane] & 31) : q;
+        const int pv = sh.gpiv[q][lane] & 31;
         used |= 1u << pv;
 #pragma unroll
         for (int c = 0; c < NC; c++) {
@@ -1091,7 +1074,7 @@ __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, 
     const Blk& a0 = (k != 0) ? sh.srv.a1 : sh.srv.y[par][0];
 #pragma unroll
     for (int c = 0; c < 4; c++) a[c] = a0[lane][warp * 4 + c];
-    if (!(p.pivot ? gj_ahead<true>(p, sh, a, t) : gj_ahead<false>(p, sh, a, t))) sh.gj_fail = 1;
+    if (!gj_ahead(p, sh, a, t)) sh.gj_fail = 1;
     if (t == 0) {
       trace_ev(p, s, kTrSrvGJ);
       sh.panel_abort = tcons_ok ? 0 : !wait_ge(p, sy.t_cons + par, ntiles * (s >> 1));
@@ -1113,7 +1096,6 @@ __device__ void server_role(const PersistParams& p, Shared& sh, const Sync& sy, 
       trace_ev(p, s, kTrPanelTout);
     }
   }
-  if (t == 0 && sh.gj_weak) atomicOr(p.status, kStatusWeakPivot);
 }
 
 // ---------------------------------------------------------------------------
@@ -1278,7 +1260,6 @@ __global__ void __launch_bounds__(Cfg<BM, BN>::Threads, 1) k_persist(PersistPara
     sh.ysig[0] = sh.ysig[1] = -1;
     sh.asig[0] = sh.asig[1] = -1;
     sh.ycons = -1;
-    sh.gj_weak = 0;
   }
   __syncthreads();
   const bool server = blockIdx.x == (unsigned)(p.TR * p.TC);
@@ -1425,7 +1406,6 @@ __global__ void __launch_bounds__(Cfg<BM, BN>::Threads, 1)
           sh.ysig[0] = sh.ysig[1] = -1;
           sh.asig[0] = sh.asig[1] = -1;
           sh.ycons = -1;
-          sh.gj_weak = 0;
         }
       }
       bar_sync(kBarGang, kAll);

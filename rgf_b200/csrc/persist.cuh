@@ -39,8 +39,6 @@ struct PersistParams {
   unsigned long long* probe_max;  // bits of max |G_n M_n v - v| (non-negative double)
   long long timeout_cycles;
   int withhold_t;        // test hook: the T-server never releases its T flag
-  int pivot;             // 1: partial pivoting inside each 32x32 pivot block; 0: diagonal pivots
-                         // (checked against the column maximum, kStatusWeakPivot)
   // optional per-step event timestamps (%globaltimer, ns) for the first
   // trace_steps steps: trace[(cta * trace_steps + s) * kTraceEvents + e]
   unsigned long long* trace;

@@ -99,8 +99,7 @@ struct rgf_handle_s {
   rgf::GangBatch* gang = nullptr;
   bool gang_submitted = false;
   int engine_used = 0;     // engine of the last call's final run
-  int fallback = 0;        // recomputes of the last call after a rejected result (0-2)
-  int pivot_tier = 0;      // persistent engine: 0 diagonal pivots (checked), 1 in-block partial pivoting
+  int fallback = 0;        // 1: the persistent engine's result was rejected and recomputed
   double probe_first = 0;  // probe residual of the rejected run
   // non-null: every workspace buffer is carved from this arena and nothing is
   // ever allocated (the handle of rgf_smatrix_2d_noalloc)
@@ -523,10 +522,8 @@ void gang_leave(GangBatch* g) {
 // RGF_ERR_ILLCOND (MATLAB's inv would warn "close to singular").
 constexpr double kProbeRetry = 1e-10;
 constexpr double kProbeIllcond = 1e-8;
-// internal statuses of smatrix_run: recompute with the persistent engine's
-// in-block pivoting, or with engine 1
+// internal status of smatrix_run: recompute with engine 1
 constexpr rgf_status kRetryWholeColumn = static_cast<rgf_status>(1000);
-constexpr rgf_status kRetryPivoting = static_cast<rgf_status>(1001);
 
 // Segment sweep of an L-split S-matrix: the slices [0, cut) swept from the
 // left lead (side 0) or [cut, L) from the right lead (side 1), carrying only
@@ -846,7 +843,6 @@ rgf_status smatrix_run(rgf_handle h, const Problem& p, const rgf_request* req, c
       // releases its T flag, so every dependent wait runs out
       const char* wh_env = getenv("RGF_TEST_WITHHOLD_T");
       pp.withhold_t = (wh_env && atoi(wh_env) == 1) ? 1 : 0;
-      pp.pivot = h->pivot_tier;
       pp.trace = nullptr;  // per-step event timestamps: a development aid, off in the library
       pp.trace_steps = 0;
       const bool timed = prof_every > 0;
@@ -869,7 +865,7 @@ rgf_status smatrix_run(rgf_handle h, const Problem& p, const rgf_request* req, c
         }
       }
       cudaError_t e;
-      if (h->gang && !h->gang_submitted && BMp == 96) {
+      if (h->gang && BMp == 96) {
         // one launch for the whole batch (96 x 96 tiles): hand the sweep to
         // the gang launch and wait until it has run; a structure that needs
         // smaller tiles sweeps on its own before the gang launch
@@ -1102,8 +1098,7 @@ rgf_status smatrix_run(rgf_handle h, const Problem& p, const rgf_request* req, c
   // the persistent engine pivots inside each 32 x 32 block only: a zero or
   // non-finite pivot there, or a slice inverse whose probe residual is not
   // at round-off level, sends the whole call to the per-step engine
-  if (ran_persist && ((hstatus & (kStatusSingular | kStatusWeakPivot)) || !(h->probe <= kProbeRetry)))
-    return h->pivot_tier == 0 ? kRetryPivoting : kRetryWholeColumn;
+  if (ran_persist && ((hstatus & kStatusSingular) || !(h->probe <= kProbeRetry))) return kRetryWholeColumn;
   if (hstatus & kStatusSingular) {
     set_error("a slice matrix is singular (zero pivot under partial pivoting)");
     return RGF_ERR_SINGULAR;
@@ -1128,18 +1123,12 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
                    int64_t ldS, rgf_channels* ch, const GradReq* gr = nullptr, const SegReq* seg = nullptr) {
   const int engine = (opt && opt->engine == 1) ? 1 : 0;
   h->fallback = 0;
-  h->pivot_tier = 0;  // the persistent engine first with diagonal pivots
   rgf_status st = smatrix_run(h, p, req, opt, S, ldS, ch, gr, engine, seg);
-  if (st == kRetryPivoting) {
-    h->probe_first = h->probe;
-    h->fallback = 1;
-    h->pivot_tier = 1;  // in-block partial pivoting
-    st = smatrix_run(h, p, req, opt, S, ldS, ch, gr, 0, seg);
-  }
   if (st == kRetryWholeColumn) {
-    if (!h->fallback) h->probe_first = h->probe;
-    h->fallback++;
+    const double probe0 = h->probe;
     st = smatrix_run(h, p, req, opt, S, ldS, ch, gr, 1, seg);
+    h->fallback = 1;
+    h->probe_first = probe0;
   }
   return st;
 }

@@ -64,7 +64,6 @@ enum : int {
   kStatusSingular = 1,
   kStatusNonfinite = 2,
   kStatusTimeout = 4,
-  kStatusWeakPivot = 8,  // a diagonal pivot of the unpivoted sweep failed its magnitude check
 };
 
 // thread-local last error (rgf_api.cu)
