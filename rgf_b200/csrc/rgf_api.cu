@@ -865,7 +865,7 @@ rgf_status smatrix_run(rgf_handle h, const Problem& p, const rgf_request* req, c
         }
       }
       cudaError_t e;
-      if (h->gang && BMp == 96) {
+      if (h->gang && !h->gang_submitted && BMp == 96) {
         // one launch for the whole batch (96 x 96 tiles): hand the sweep to
         // the gang launch and wait until it has run; a structure that needs
         // smaller tiles sweeps on its own before the gang launch
