@@ -18,6 +18,7 @@
 #include <string>
 #include <chrono>
 #include <condition_variable>
+#include <memory>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -1411,42 +1412,55 @@ static rgf_status batch_one_launch(rgf_handle h, int64_t count, const rgf_syst2d
                                    rgf_status* statuses) {
   std::vector<rgf_status> res(count, RGF_OK);
   std::vector<std::string> msg(count);
-  int64_t launches = 0;
-  for (int64_t c0 = 0; c0 < count; c0 += kGangChunk) {
-    const int64_t n = std::min(kGangChunk, count - c0);
-    GangBatch g;
-    g.pending = (int)n;
-    g.device = h->device;
-    g.sms = h->sms;
-    g.stream = h->stream;
-    std::vector<rgf_handle> ws(n, nullptr);
-    std::vector<std::thread> pool;
-    for (int64_t i = 0; i < n; i++) {
-      rgf_status st = rgf_create(h->device, &ws[i]);
-      if (st != RGF_OK) {
-        res[c0 + i] = st;
-        msg[c0 + i] = tl_err;
-        std::lock_guard<std::mutex> lock(g.mu);
-        gang_arrive_locked(&g);
-        continue;
-      }
-      ws[i]->gang = &g;
-      ws[i]->tile_rmax = h->tile_rmax;
-      ws[i]->tile_bm = h->tile_bm;
-      pool.emplace_back([&, i] {
-        rgf_handle w = ws[i];
-        cudaSetDevice(w->device);
-        const int64_t k = c0 + i;
-        res[k] = smatrix(w, problem2d(&systs[k]), &reqs[k], opt, S[k], ldS[k], nullptr);
-        if (res[k] != RGF_OK) msg[k] = tl_err;
-        if (!w->gang_submitted) gang_leave(&g);
-      });
-    }
-    for (auto& th : pool) th.join();
-    launches += g.launches;
-    for (rgf_handle w : ws)
-      if (w) rgf_destroy(w);
+  // more than kGangChunk structures: several launches, each with a share of
+  // every size (structures dealt round-robin in order of cost); all threads
+  // run at once, so one launch's set-up overlaps another's sweeps
+  const int64_t nch = (count + kGangChunk - 1) / kGangChunk;
+  std::vector<int64_t> order(count);
+  for (int64_t i = 0; i < count; i++) order[i] = i;
+  std::vector<double> cost(count);
+  for (int64_t i = 0; i < count; i++) {
+    const double N = (double)systs[i].ny;
+    cost[i] = (double)std::max<int64_t>(systs[i].nx, 1) * N * N * N;
   }
+  std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) { return cost[x] > cost[y]; });
+  std::vector<std::unique_ptr<GangBatch>> gb(nch);
+  for (int64_t c = 0; c < nch; c++) {
+    gb[c].reset(new GangBatch());
+    gb[c]->device = h->device;
+    gb[c]->sms = h->sms;
+    gb[c]->stream = h->stream;
+  }
+  for (int64_t r = 0; r < count; r++) gb[r % nch]->pending++;
+  std::vector<rgf_handle> ws(count, nullptr);
+  std::vector<std::thread> pool;
+  for (int64_t r = 0; r < count; r++) {
+    const int64_t k = order[r];
+    GangBatch* g = gb[r % nch].get();
+    rgf_status st = rgf_create(h->device, &ws[k]);
+    if (st != RGF_OK) {
+      res[k] = st;
+      msg[k] = tl_err;
+      std::lock_guard<std::mutex> lock(g->mu);
+      gang_arrive_locked(g);
+      continue;
+    }
+    ws[k]->gang = g;
+    ws[k]->tile_rmax = h->tile_rmax;
+    ws[k]->tile_bm = h->tile_bm;
+    pool.emplace_back([&, k, g] {
+      rgf_handle w = ws[k];
+      cudaSetDevice(w->device);
+      res[k] = smatrix(w, problem2d(&systs[k]), &reqs[k], opt, S[k], ldS[k], nullptr);
+      if (res[k] != RGF_OK) msg[k] = tl_err;
+      if (!w->gang_submitted) gang_leave(g);
+    });
+  }
+  for (auto& th : pool) th.join();
+  int64_t launches = 0;
+  for (auto& g : gb) launches += g->launches;
+  for (rgf_handle w : ws)
+    if (w) rgf_destroy(w);
   h->launches = launches;  // persistent (gang) launches of the call
   rgf_status first = RGF_OK;
   for (int64_t i = 0; i < count; i++) {
