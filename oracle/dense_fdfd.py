@@ -18,7 +18,7 @@ from __future__ import annotations
 import numpy as np
 
 from .rgf_ref import (_delta_matrix, build_laplacian_1d, parse_channel_request,
-                      setup_channels)
+                      setup_channels, setup_channels_3D)
 
 
 def smatrix_dense_2d(syst, out, in_):
@@ -38,14 +38,39 @@ def _dense_2d(syst, out, in_, fields):
     ny, nx = eps.shape
     k0dx = syst["k0dx"]
     ch = setup_channels(int(ny), syst["yBC"], k0dx, syst["epsilon_L"], syst["epsilon_R"])
-    chL, chR = ch["L"], ch["R"]
+    phi = ch["fun_phi"](ch["kydx"])
+    A0 = -build_laplacian_1d(int(ny), syst["yBC"]) + 2 * np.eye(ny)
+    return _dense(phi, ch["L"], ch["R"], ch["L"]["kxdx"], ch["R"]["kxdx"], A0, k0dx, eps, out, in_, fields)
+
+
+def fields_dense_3d(syst, out, in_):
+    """(S, psi) of cal_smatrix_RGF_3D from a dense solve: psi[:, n, b] at the
+    nx*ny sites (x fastest) of slice n, as fields_dense_2d."""
+    eps = np.asarray(syst["epsilon"], dtype=complex)
+    if eps.ndim == 2:
+        eps = eps[:, :, None]
+    nx, ny, nz = eps.shape
+    k0dx = syst["k0dx"]
+    xyBC = syst["xyBC"]
+    ch = setup_channels_3D(int(nx), int(ny), xyBC, k0dx, syst["epsilon_L"], syst["epsilon_R"])
+    kxf, kyf = ch["kxdx"].ravel(order="F"), ch["kydx"].ravel(order="F")
+    phi = np.stack([ch["fun_phi"](kxf[a], kyf[a]).ravel(order="F") for a in range(nx * ny)], axis=1)
+    if isinstance(xyBC, str):
+        xBC = yBC = xyBC
+    else:
+        xBC, yBC = (float(np.real(v)) for v in np.asarray(xyBC).ravel()[:2])
+    A0 = (-np.kron(np.eye(ny), build_laplacian_1d(int(nx), xBC)) - np.kron(build_laplacian_1d(int(ny), yBC), np.eye(nx))
+          + 2 * np.eye(nx * ny))
+    return _dense(phi, ch["L"], ch["R"], ch["L"]["kzdx"].ravel(order="F"), ch["R"]["kzdx"].ravel(order="F"), A0, k0dx,
+                  eps.reshape((nx * ny, nz), order="F"), out, in_, True)
+
+
+def _dense(phi, chL, chR, kxL, kxR, A0, k0dx, eps, out, in_, fields):
+    N, nx = eps.shape
     iiL, iiR = parse_channel_request(in_, "in", chL["N_prop"], chR["N_prop"])
     ioL, ioR = parse_channel_request(out, "out", chL["N_prop"], chR["N_prop"])
-    phi = ch["fun_phi"](ch["kydx"])
-    N = ny
-    G0L = (phi * np.exp(1j * chL["kxdx"])[None, :]) @ phi.conj().T
-    G0R = (phi * np.exp(1j * chR["kxdx"])[None, :]) @ phi.conj().T
-    A0 = -build_laplacian_1d(int(ny), syst["yBC"]) + 2 * np.eye(ny)
+    G0L = (phi * np.exp(1j * kxL)[None, :]) @ phi.conj().T
+    G0R = (phi * np.exp(1j * kxR)[None, :]) @ phi.conj().T
     nsite = nx + 2
     H = np.zeros((nsite * N, nsite * N), dtype=complex)
 

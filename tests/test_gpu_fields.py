@@ -61,17 +61,18 @@ def test_fields_energy_flux_real_eps():
     assert np.abs(amp - amp[0]).max() <= 1e-12 * amp[0]
 
 
-def test_fields_3d_consistent_with_2d():
-    """3D with a size-1 x axis and periodic BC is the 2D problem (the n = 1
-    Laplacian is zero)."""
-    rng = np.random.default_rng(14)
-    eps2 = 1 + 2 * rng.random((8, 6))
-    s2 = dict(epsilon=eps2, epsilon_L=1.0, epsilon_R=1.0, k0dx=1.0, yBC="periodic")
-    s3 = dict(epsilon=eps2[None, :, :], epsilon_L=1.0, epsilon_R=1.0, k0dx=1.0, xyBC="periodic")
-    S2, p2 = rgf_b200.fields_RGF(s2, ["left", "right"], ["left"])
-    S3, p3 = rgf_b200.fields_RGF_3D(s3, ["left", "right"], ["left"])
-    assert p3.shape == (1, 8, 6, p2.shape[2])
-    # channel order may differ between the 2D and 3D set-ups: compare the
-    # field space spanned by the inputs through S's unitary structure
-    assert np.linalg.norm(S3) == pytest.approx(np.linalg.norm(S2), rel=1e-12)
-    assert np.linalg.norm(p3) == pytest.approx(np.linalg.norm(p2), rel=1e-11)
+@pytest.mark.parametrize("bc,out,inp", [
+    ("periodic", ["left", "right"], ["left", "right"]),
+    ("Dirichlet", ["right"], ["left"]),
+    ([0.3, -0.2], {"ind_out_L": [1]}, {"ind_in_R": [2, 1]}),
+])
+def test_fields_3d_match_dense_solve(bc, out, inp):
+    """3D: psi[x, y, n, b] against the dense solve of the whole operator."""
+    from oracle.dense_fdfd import fields_dense_3d
+    rng = np.random.default_rng(15)
+    syst = dict(epsilon=1 + rng.random((4, 3, 5)), epsilon_L=1.0, epsilon_R=1.3, k0dx=2 * np.pi / 5, xyBC=bc)
+    S, psi = rgf_b200.fields_RGF_3D(syst, out, inp, checkpoint=2)
+    S0, psi0 = fields_dense_3d(syst, out, inp)
+    assert np.linalg.norm(S - S0) <= 1e-11 * np.linalg.norm(S0)
+    assert psi.shape == (4, 3, 5, psi0.shape[2])
+    assert relmax(psi.reshape((12, 5, -1), order="F"), psi0) <= TOL
