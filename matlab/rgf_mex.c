@@ -9,6 +9,7 @@
  *   [S, ch] = rgf_mex('smatrix2d', syst, out, in)        cal_smatrix_RGF
  *   [S, ch] = rgf_mex('smatrix3d', syst, out, in)        cal_smatrix_RGF_3D
  *   [S, g]  = rgf_mex('grad2d', syst, out, in, D)        dS/d eps contracted with D
+ *   [S, psi] = rgf_mex('fields2d', syst, out, in)        fields G B at every slice, [ny, nx, n_in]
  *   ch      = rgf_mex('channels2d', ny, BC, k0dx, epsL, epsR)
  *   ch      = rgf_mex('channels3d', nx, ny, BC, k0dx, epsL, epsR)
  *   A       = rgf_mex('laplacian', n, BC)                 build_laplacian_1d (dense)
@@ -238,8 +239,9 @@ static mxArray* chbuf_struct(const chbuf* b, int64_t N, int dim) {
   return s;
 }
 
+/* grad: 1 = gradient (prhs[4] = D), 2 = fields */
 static void smatrix_cmd(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[], int dim, int grad) {
-  if (nrhs < 4 + grad) mexErrMsgIdAndTxt("rgf:arg", "not enough input arguments");
+  if (nrhs < 4 + (grad == 1)) mexErrMsgIdAndTxt("rgf:arg", "not enough input arguments");
   const mxArray* syst = prhs[1];
   if (!mxIsStruct(syst)) mexErrMsgIdAndTxt("rgf:arg", "syst must be a structure");
   const mxArray* e = field(syst, "epsilon");
@@ -290,6 +292,17 @@ static void smatrix_cmd(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs
   }
   plhs[0] = mxCreateDoubleMatrix(no, ni, mxCOMPLEX);
   rgf_cplx* S = (rgf_cplx*)mxGetComplexDoubles(plhs[0]);
+  if (grad == 2) {  /* fields: [ny, nx, n_in] (2D) */
+    const mwSize fd[3] = {(mwSize)N, (mwSize)L, (mwSize)ni};
+    mxArray* psi = mxCreateNumericArray(3, fd, mxDOUBLE_CLASS, mxCOMPLEX);
+    rgf_status st = rgf_fields_2d(H, &s2, &req, NULL, no ? S : NULL, no > 0 ? no : 1,
+                                  (rgf_cplx*)mxGetComplexDoubles(psi), 0);
+    if (tmp) mxDestroyArray(tmp);
+    check(st);
+    if (nlhs > 1) plhs[1] = psi;
+    else mxDestroyArray(psi);
+    return;
+  }
   if (grad) {
     const mxArray* Da = prhs[4];
     if (!mxIsDouble(Da) || mxGetM(Da) != (mwSize)no || mxGetN(Da) != (mwSize)ni)
@@ -332,6 +345,8 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
     smatrix_cmd(nlhs, plhs, nrhs, prhs, 3, 0);
   } else if (!strcmp(cmd, "grad2d")) {
     smatrix_cmd(nlhs, plhs, nrhs, prhs, 2, 1);
+  } else if (!strcmp(cmd, "fields2d")) {
+    smatrix_cmd(nlhs, plhs, nrhs, prhs, 2, 2);
   } else if (!strcmp(cmd, "channels2d") || !strcmp(cmd, "channels3d")) {
     const int dim = cmd[8] == '3' ? 3 : 2;
     const int a0 = dim == 3 ? 2 : 1;

@@ -170,3 +170,21 @@ def test_gradient_through_gateway():
     finally:
         bridge.destroy(S)
         bridge.destroy(g)
+
+
+@pytest.mark.gpu
+def test_fields_through_gateway():
+    from oracle.dense_fdfd import fields_dense_2d
+    rng = np.random.default_rng(9)
+    syst = dict(epsilon=1 + 2 * rng.random((10, 6)), epsilon_L=1.0, epsilon_R=1.2, k0dx=1.0, yBC="Neumann")
+    out, inp = ["left", "right"], {"ind_in_R": [1, 2]}
+    (S, psi), _ = bridge.call(2, "fields2d", syst_mx(syst), mx_request(out), mx_request(inp))
+    try:
+        S0, psi0 = fields_dense_2d(syst, out, inp)
+        assert rel(bridge.from_mx(S), S0) <= 1e-11
+        p = bridge.from_mx(psi)
+        assert p.shape == (10, 6, 2)
+        assert np.abs(p - psi0).max() <= 1e-11 * np.abs(psi0).max()
+    finally:
+        bridge.destroy(S)
+        bridge.destroy(psi)
