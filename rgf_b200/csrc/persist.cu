@@ -255,71 +255,6 @@ struct MathTile {
   __device__ int col(int ni, int h) const { return c_base + ni * 8 + (lane & 3) * 2 + h; }
 };
 
-__device__ __forceinline__ double2 assemble_elem(const PersistParams& p, int64_t i, int64_t j, double2 v,
-                                                 const double2* eps_next) {
-  if (j < p.N) {
-    if (i < p.N) {
-      double2 a = cneg(v);
-#pragma unroll
-      for (int q = 0; q < kMaxStencil; q++)
-        if (p.st_col[i * kMaxStencil + q] == j) a = cadd(a, p.st_val[i * kMaxStencil + q]);
-      if (i == j) a = csub(a, cmul(p.k2, eps_next[i]));
-      return a;
-    }
-    return cneg(v);  // -Z rows
-  }
-  return v;  // X columns and the Y block are carried unchanged
-}
-
-// Slice boundary on this CTA's tile of W (global memory): probe check
-// (p2 = G_n M_n v against v), the snapshot of W after the slice when `snap`
-// is given (same layout as W, probe columns excepted) and, when eps_next is
-// given, the assembly of the next slice matrix: top-left A_{n+1} - G_n, -Z
-// rows, probe pair p1 = v, p2 = A_{n+1} v - G_n v.  Returns the largest probe
-// residual seen.
-template <int BM, int BN>
-__device__ double boundary_pass(const PersistParams& p, int I, int Cq, int tid, int nthreads,
-                                const double2* eps_next, double2* snap) {
-  double pmax = 0.0;
-  const int64_t r0 = (int64_t)I * BM, c0 = (int64_t)Cq * BN;
-  const int pc1 = p.pc1;
-  for (int e = tid; e < BM * BN; e += nthreads) {
-    const int64_t i = r0 + e / BN, j = c0 + e % BN;
-    if (i >= p.R || j >= p.C) continue;
-    double2* w = p.M + i * p.ldm + j;
-    if (pc1 >= 0 && (j == pc1 || j == pc1 + 1)) {
-      if (j != pc1) continue;  // the thread of column p1 handles the pair
-      double2* w2 = w + 1;
-      if (i < p.N) {
-        const double2 v = probe_v(i);
-        const double2 d = csub(__ldcg(w2), v);
-        const double rr = sqrt(cabs2(d));
-        pmax = (rr == rr) ? fmax(pmax, rr) : INFINITY;  // fmax would drop a NaN
-        if (eps_next) {
-          double2 Av = cmk(0.0, 0.0);
-          for (int q = 0; q < kMaxStencil; q++) {
-            const int cq = p.st_col[i * kMaxStencil + q];
-            if (cq >= 0) Av = cadd(Av, cmul(p.st_val[i * kMaxStencil + q], probe_v(cq)));
-          }
-          Av = csub(Av, cmul(cmul(p.k2, eps_next[i]), v));
-          const double2 Gv = __ldcg(w);
-          __stcg(w, v);
-          __stcg(w2, csub(Av, Gv));
-        }
-      } else if (eps_next) {
-        __stcg(w, cmk(0.0, 0.0));
-        __stcg(w2, cmk(0.0, 0.0));
-      }
-      continue;
-    }
-    if (!eps_next && !snap) continue;
-    const double2 v = __ldcg(w);
-    if (snap) __stcg(snap + i * p.ldm + j, v);
-    if (eps_next) __stcg(w, assemble_elem(p, i, j, v, eps_next));
-  }
-  return pmax;
-}
-
 template <int BM, int BN>
 __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, int I, int Cq) {
   using Tile = MathTile<BM, BN>;
@@ -392,6 +327,103 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
           const int i = t.row(mi), j = t.col(ni, h);
           if (i < p.R && j < p.C) __stcg(p.M + (int64_t)i * p.ldm + j, cmk(t.acc[mi][ni][h], t.acc[mi][ni][2 + h]));
         }
+  };
+  // Slice boundary on the register tile: probe check (p2 = G_n M_n v against
+  // v), the snapshot of W after the slice when `snap` is given (layout of W,
+  // probe columns excepted) and, when eps_next is given, the next slice
+  // matrix in place: top-left A_{n+1} - G_n, -Z rows, X columns and the Y
+  // block unchanged, probe pair p1 = v, p2 = A_{n+1} v - G_n v.  Each thread
+  // works on its own accumulators only.  The probe pair is the column pair
+  // (pc1, pc1 + 1), pc1 even, so one thread holds both as h = 0, 1.
+  // Returns the largest probe residual this thread saw.
+  auto boundary_regs = [&](const double2* eps_next, double2* snap) {
+    double pmax = 0.0;
+    // the probe pair of each row goes through a small local array, so that
+    // its (long) arithmetic is instantiated once, not once per accumulator
+    double2 pr[MI][2];
+    unsigned has = 0;
+#pragma unroll
+    for (int mi = 0; mi < MI; mi++) {
+      const int i = t.row(mi);
+      if (i >= p.R) continue;
+      const bool top = i < p.N;
+      const double2 ke = (eps_next && top) ? cmul(p.k2, __ldg(eps_next + i)) : cmk(0.0, 0.0);
+#pragma unroll
+      for (int ni = 0; ni < NI; ni++) {
+        const int j0c = t.col(ni, 0);  // even; j0c + 1 is the h = 1 column
+        if (j0c >= p.C) continue;
+        double* a = t.acc[mi][ni];
+        if (j0c == p.pc1) {
+          pr[mi][0] = cmk(a[0], a[2]);
+          pr[mi][1] = cmk(a[1], a[3]);
+          has |= 1u << mi;
+          continue;
+        }
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const int j = j0c + h;
+          if (j >= p.C) continue;
+          if (snap) __stcg(snap + (int64_t)i * p.ldm + j, cmk(a[h], a[2 + h]));
+          if (!eps_next || j >= p.N) continue;  // X columns and the Y block are carried unchanged
+          a[h] = -a[h];  // -G_n, or the -Z rows
+          a[2 + h] = -a[2 + h];
+          if (i == j) {
+            a[h] -= ke.x;
+            a[2 + h] -= ke.y;
+          }
+        }
+      }
+      // + A0 (stencil entries of row i), one entry at a time
+      if (!eps_next || !top) continue;
+#pragma unroll 1
+      for (int q = 0; q < kMaxStencil; q++) {
+        const int cq = __ldg(p.st_col + (int64_t)i * kMaxStencil + q);
+        if (cq < 0) continue;
+        const double2 v = __ldg(p.st_val + (int64_t)i * kMaxStencil + q);
+#pragma unroll
+        for (int ni = 0; ni < NI; ni++)
+#pragma unroll
+          for (int h = 0; h < 2; h++)
+            if (cq == t.col(ni, h) && cq != p.pc1 && cq != p.pc1 + 1) {
+              t.acc[mi][ni][h] += v.x;
+              t.acc[mi][ni][2 + h] += v.y;
+            }
+      }
+    }
+    if (has == 0u) return pmax;
+#pragma unroll 1
+    for (int mi = 0; mi < MI; mi++) {
+      if (!((has >> mi) & 1u)) continue;
+      const int i = t.row(mi);
+      if (i < p.N) {
+        const double2 v = probe_v(i);
+        const double2 d = csub(pr[mi][1], v);
+        const double rr = sqrt(cabs2(d));
+        pmax = (rr == rr) ? fmax(pmax, rr) : INFINITY;  // fmax would drop a NaN
+        if (eps_next) {
+          double2 Av = csub(cmk(0.0, 0.0), cmul(cmul(p.k2, __ldg(eps_next + i)), v));
+          for (int q = 0; q < kMaxStencil; q++) {
+            const int cq = __ldg(p.st_col + (int64_t)i * kMaxStencil + q);
+            if (cq >= 0) Av = cadd(Av, cmul(__ldg(p.st_val + (int64_t)i * kMaxStencil + q), probe_v(cq)));
+          }
+          pr[mi][1] = csub(Av, pr[mi][0]);
+          pr[mi][0] = v;
+        }
+      } else if (eps_next) {
+        pr[mi][0] = pr[mi][1] = cmk(0.0, 0.0);
+      }
+    }
+#pragma unroll
+    for (int mi = 0; mi < MI; mi++)
+#pragma unroll
+      for (int ni = 0; ni < NI; ni++)
+        if (((has >> mi) & 1u) && t.col(ni, 0) == p.pc1) {
+          t.acc[mi][ni][0] = pr[mi][0].x;
+          t.acc[mi][ni][2] = pr[mi][0].y;
+          t.acc[mi][ni][1] = pr[mi][1].x;
+          t.acc[mi][ni][3] = pr[mi][1].y;
+        }
+    return pmax;
   };
   // rank-32 update of the whole warp tile: first halves of every complex
   // product, then the dependent second halves
@@ -676,21 +708,15 @@ __device__ void math_role(const PersistParams& p, Shared& sh, const Sync& sy, in
     if (!last_block) publish(s1, false);
     if (tid == 0) trace_ev(p, s, kTrMathDone);
     if (last_block) {
-      // slice boundary: the tile goes to its home in W, the probe is checked
-      // and the next slice matrix A_{n+1} - G_n is assembled there with plain
-      // code (keeps the accumulator-resident loop free of spills), then the
-      // tile is reloaded and the first pieces of slice n+1 published.
-      store_tile();
-      bar_sync(kBarMath, kMathThreads);
+      // slice boundary: probe check and the next slice matrix A_{n+1} - G_n
+      // in the registers, then the first pieces of slice n+1 published; after
+      // the last slice the tile goes to its home in W
       const double2* eps_next = slice_end ? p.eps + (p.eps_first + (int64_t)(n + 1) * p.eps_step) * p.N : nullptr;
       double2* snap = (p.snap && (n % p.snap_mod) == p.snap_mod - 1) ? p.snap + (int64_t)(n / p.snap_mod) * p.snap_ld
                                                                      : nullptr;
-      probe_max = fmax(probe_max, boundary_pass<BM, BN>(p, I, Cq, tid, kMathThreads, eps_next, snap));
-      bar_sync(kBarMath, kMathThreads);
-      if (slice_end) {
-        load_tile();
-        publish(s1, true);
-      }
+      probe_max = fmax(probe_max, boundary_regs(eps_next, snap));
+      if (slice_end) publish(s1, true);
+      else store_tile();
     }
   }
   for (int off = 16; off > 0; off >>= 1) probe_max = fmax(probe_max, __shfl_xor_sync(kFull, probe_max, off));
