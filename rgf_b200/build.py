@@ -83,7 +83,7 @@ def build_selftest(verbose: bool = False, force: bool = False) -> Path:
     """Unit-test kernels for device functions without a C-ABI entry (tests only)."""
     if not SELFTEST_SRC.exists():
         return SELFTEST_OUT
-    deps = [SELFTEST_SRC, CSRC / "recip.cuh", CSRC / "rgf_internal.cuh"]
+    deps = [SELFTEST_SRC, CSRC / "recip.cuh", CSRC / "rgf_internal.cuh", CSRC / "tc32.cuh"]
     if SELFTEST_OUT.exists() and not force and SELFTEST_OUT.stat().st_mtime >= max(p.stat().st_mtime for p in deps):
         return SELFTEST_OUT
     tmp = SELFTEST_OUT.with_suffix(".so.tmp")
