@@ -74,7 +74,13 @@ typedef enum {
 
 /* Numeric form of the slice recursion. */
 typedef enum {
-  RGF_FP64 = 0 /* complex FP64 throughout (the drop-in form) */
+  RGF_FP64 = 0,  /* complex FP64 throughout (the drop-in form) */
+  RGF_TF32X3 = 1 /* split precision: every slice inverse factored in FP32 with 3xTF32
+                    tensor-core updates (tcgen05), S won back by FP64 iterative
+                    refinement of the block-tridiagonal solve against the FP64
+                    operator; falls back to RGF_FP64 when the refinement does not
+                    converge (rgf_last_refinement tells).  S-matrices only
+                    (rgf_smatrix_2d/3d and the pipelined batch).              */
 } rgf_precision;
 
 /* Value of n_* in rgf_request meaning "all propagating channels on that side"
@@ -271,6 +277,16 @@ RGF_API rgf_status rgf_last_stats(rgf_handle h, int64_t* kernel_launches, double
  * pivot, or a probe residual above 1e-10) and recomputed with engine 1;
  * rejected_probe is that run's residual.  An addition of this library. */
 RGF_API rgf_status rgf_last_engine(rgf_handle h, int32_t* engine, int32_t* fallback, double* rejected_probe);
+/* The split-precision form (RGF_TF32X3) of the last rgf_smatrix_* call on
+ * this handle (an addition of this library; the reference has one FP64 form):
+ * form = RGF_TF32X3 when its S stands, -RGF_TF32X3 when the refinement did not
+ * converge and S was recomputed in FP64, RGF_FP64 when it was not asked for;
+ * the number of refinement passes (the first solve included), the relative
+ * size of the last correction (max over the whole solution and its first and
+ * last slices), and the device time of the FP32 factorization and of all
+ * solves (ms). */
+RGF_API rgf_status rgf_last_refinement(rgf_handle h, int32_t* form, int32_t* iterations, double* last_change,
+                                       double* factor_ms, double* solve_ms);
 /* Sampled timing of the dominant kernel of the last rgf_smatrix_* call made
  * with opt->profile > 0: number of timed launches, their summed duration (ms),
  * the algorithmic flops of one such launch, and its name. */

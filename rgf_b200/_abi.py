@@ -25,6 +25,7 @@ STATUS_NAMES = {0: "RGF_OK", 1: "RGF_ERR_ARG", 2: "RGF_ERR_NONFINITE", 3: "RGF_E
 BC_PERIODIC, BC_DIRICHLET, BC_NEUMANN, BC_DIRICHLET_NEUMANN, BC_NEUMANN_DIRICHLET, BC_BLOCH = range(6)
 RGF_ALL = -1
 RGF_FP64 = 0
+RGF_TF32X3 = 1  # split-precision form (3xTF32 factorization + FP64 refinement)
 RGF_NOALLOC_SCRATCH_BYTES = 32 << 20  # include/rgf.h
 RGF_NOALLOC_SCRATCH_BYTES = 32 << 20  # include/rgf.h
 
@@ -104,6 +105,8 @@ SIGNATURES = {
     "rgf_version": (c_char_p, []),
     "rgf_last_stats": (c_int, [c_void_p, POINTER(c_int64), POINTER(c_double)]),
     "rgf_last_engine": (c_int, [c_void_p, POINTER(c_int32), POINTER(c_int32), POINTER(c_double)]),
+    "rgf_last_refinement": (c_int, [c_void_p, POINTER(c_int32), POINTER(c_int32), POINTER(c_double),
+                                    POINTER(c_double), POINTER(c_double)]),
     "rgf_last_profile": (c_int, [c_void_p, POINTER(c_int64), POINTER(c_double), POINTER(c_double), c_char_p,
                                  ctypes.c_size_t]),
     "rgf_set_stream": (c_int, [c_void_p, c_void_p]),
@@ -193,6 +196,18 @@ class Handle:
         e, f, r = c_int32(), c_int32(), c_double()
         check(self.lib.rgf_last_engine(self.h, ctypes.byref(e), ctypes.byref(f), ctypes.byref(r)))
         return int(e.value), int(f.value), float(r.value)
+
+    def refinement(self):
+        """Split-precision form of the last S-matrix call: dict with form
+        (RGF_TF32X3 when its S stands, -RGF_TF32X3 after a fallback to FP64,
+        RGF_FP64 when not asked for), iterations, last_change, factor_ms,
+        solve_ms."""
+        f, it = c_int32(), c_int32()
+        ch, fm, sm = c_double(), c_double(), c_double()
+        check(self.lib.rgf_last_refinement(self.h, ctypes.byref(f), ctypes.byref(it), ctypes.byref(ch),
+                                           ctypes.byref(fm), ctypes.byref(sm)))
+        return {"form": int(f.value), "iterations": int(it.value), "last_change": float(ch.value),
+                "factor_ms": float(fm.value), "solve_ms": float(sm.value)}
 
     def stats(self):
         n = c_int64()

@@ -21,7 +21,7 @@ SELFTEST_OUT = PKG.parent / "tests" / "cuda" / "libselftest.so"
 MEXSTUB_DIR = PKG.parent / "tests" / "mexstub"
 MEXSTUB_OUT = MEXSTUB_DIR / "libmexstub.so"
 MEX_GATEWAY = PKG.parent / "matlab" / "rgf_mex.c"
-SOURCES = ["channels.cu", "sweep.cu", "persist.cu", "rgf_api.cu"]
+SOURCES = ["channels.cu", "sweep.cu", "persist.cu", "mixed.cu", "rgf_api.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr"]

@@ -26,6 +26,7 @@
 #include "channels.cuh"
 #include "persist.cuh"
 #include "rgf_internal.cuh"
+#include "mixed.cuh"
 #include "sweep.cuh"
 
 namespace rgf {
@@ -105,6 +106,11 @@ struct rgf_handle_s {
   // non-null: every workspace buffer is carved from this arena and nothing is
   // ever allocated (the handle of rgf_smatrix_2d_noalloc)
   Arena* arena = nullptr;
+  // split-precision form (RGF_TF32X3): workspace, and what the last call did
+  DevBuf mx[kMxSlots];
+  MixedStats mx_stats;
+  int mx_form = RGF_FP64;  // form whose S the last call returned
+  int mx_fallback = 0;     // 1: the refinement did not converge and S is the FP64 form's
 };
 
 namespace {
@@ -545,8 +551,14 @@ rgf_status smatrix_run(rgf_handle h, const Problem& p, const rgf_request* req, c
   h->probe = 0.0;
   h->engine_used = engine;
   if ((st = validate_problem(p, req))) return st;
-  if (opt && opt->precision != RGF_FP64) {
-    set_error("unsupported precision form");
+  const bool want_mixed = opt && opt->precision == RGF_TF32X3;
+  if (opt && opt->precision != RGF_FP64 && !want_mixed) {
+    set_error("unsupported precision form (rgf_precision: RGF_FP64 or RGF_TF32X3)");
+    return RGF_ERR_ARG;
+  }
+  if (want_mixed && (gr || seg || h->gang || h->arena)) {
+    set_error("the split-precision form (RGF_TF32X3) computes S-matrices only: gradients, fields, segments, the "
+              "one-launch batch and rgf_smatrix_2d_noalloc take RGF_FP64");
     return RGF_ERR_ARG;
   }
   const bool S_dev = opt && opt->S_on_device;
@@ -651,6 +663,11 @@ rgf_status smatrix_run(rgf_handle h, const Problem& p, const rgf_request* req, c
   };
   size_t o_in_s = push(in_s), o_out_s = push(out_s), o_in_e = push(in_e), o_out_e = push(out_e);
   size_t o_row = push(row_of), o_col = push(col_of), o_pairs = push(pairs);
+  // S order [in_L; in_R] / [out_L; out_R] channel lists (split-precision form)
+  std::vector<int> in_lr(rq.in[0]), out_lr(rq.out[0]);
+  in_lr.insert(in_lr.end(), rq.in[1].begin(), rq.in[1].end());
+  out_lr.insert(out_lr.end(), rq.out[1].begin(), rq.out[1].end());
+  size_t o_in_lr = push(in_lr), o_out_lr = push(out_lr);
   if ((st = ensure(h, h->idx, sizeof(int) * (idx.size() + 1)))) return st;
   int* idx_d = as<int>(h->idx);
   RGF_CUDA_TRY(cudaMemcpyAsync(idx_d, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, h->stream));
@@ -692,6 +709,60 @@ rgf_status smatrix_run(rgf_handle h, const Problem& p, const rgf_request* req, c
     h->launches += 2;
   }
   if ((st = check_launch())) return st;
+
+  // (5b) the split-precision form: low-precision factorization + FP64
+  //      refinement of the whole solve; S written here unless the
+  //      refinement does not converge, in which case the FP64 form below runs
+  if (want_mixed && L > 0) {
+    MixedProblem mp;
+    mp.N = N;
+    mp.L = L;
+    mp.niL = niL;
+    mp.niR = niR;
+    mp.noL = noL;
+    mp.noR = noR;
+    mp.phi = phi;
+    for (int q = 0; q < 2; q++) {
+      mp.prop[q] = ci.side[q].prop;
+      mp.sqrtmu[q] = ci.side[q].sqrtmu;
+    }
+    mp.in_idx = idx_d + o_in_lr;
+    mp.out_idx = idx_d + o_out_lr;
+    mp.pairs = idx_d + o_pairs;
+    mp.npairs = npairs;
+    mp.G0[0] = s == 0 ? g0s : g0e;
+    mp.G0[1] = s == 0 ? g0e : g0s;
+    mp.st_col = as<int>(h->st_col);
+    mp.st_val = as<double2>(h->st_val);
+    mp.k2 = k2;
+    mp.eps = eps_d;
+    double2* Sd = S_dev ? reinterpret_cast<double2*>(S) : as<double2>(h->sdev);
+    mp.S = Sd;
+    mp.ldS = S_dev ? ldS : n_out;
+    MixedAlloc alloc = [&](int slot, size_t bytes, void** pp) -> rgf_status {
+      rgf_status e2 = ensure(h, h->mx[slot], bytes);
+      *pp = h->mx[slot].p;
+      return e2;
+    };
+    h->mx_stats = MixedStats();
+    st = smatrix_mixed(mp, alloc, h->stream, &h->mx_stats, &h->launches);
+    if (st == RGF_OK) {
+      if (!S_dev)
+        RGF_CUDA_TRY(cudaMemcpy2DAsync(S, sizeof(rgf_cplx) * ldS, Sd, sizeof(double2) * n_out,
+                                       sizeof(double2) * n_out, n_in, cudaMemcpyDeviceToHost, h->stream));
+      int hstatus = 0;
+      RGF_CUDA_TRY(cudaMemcpyAsync(&hstatus, status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+      RGF_CUDA_TRY(cudaStreamSynchronize(h->stream));
+      if (hstatus & kStatusNonfinite) {
+        set_error("syst.epsilon contains NaN or Inf");
+        return RGF_ERR_NONFINITE;
+      }
+      h->mx_form = RGF_TF32X3;
+      return copy_channels_out(h, tr, ci, ch);
+    }
+    if (st != kMixedNotConverged) return st;
+    h->mx_fallback = 1;  // S from the FP64 form
+  }
 
   // (6) initial augmented matrix
   double2* M = as<double2>(h->aug);
@@ -1124,10 +1195,14 @@ rgf_status smatrix(rgf_handle h, const Problem& p, const rgf_request* req, const
                    int64_t ldS, rgf_channels* ch, const GradReq* gr = nullptr, const SegReq* seg = nullptr) {
   const int engine = (opt && opt->engine == 1) ? 1 : 0;
   h->fallback = 0;
+  h->mx_form = RGF_FP64;
+  h->mx_fallback = 0;
   rgf_status st = smatrix_run(h, p, req, opt, S, ldS, ch, gr, engine, seg);
   if (st == kRetryWholeColumn) {
     const double probe0 = h->probe;
-    st = smatrix_run(h, p, req, opt, S, ldS, ch, gr, 1, seg);
+    rgf_options o2 = opt ? *opt : rgf_options{};
+    o2.precision = RGF_FP64;  // a split-precision attempt, if any, has already been made
+    st = smatrix_run(h, p, req, &o2, S, ldS, ch, gr, 1, seg);
     h->fallback = 1;
     h->probe_first = probe0;
   }
@@ -1374,6 +1449,8 @@ rgf_status rgf_destroy(rgf_handle h) {
                     &h->gg,     &h->gf,     &h->segs};
   for (DevBuf* b : bufs)
     if (b->p) cudaFree(b->p);
+  for (DevBuf& b : h->mx)
+    if (b.p) cudaFree(b.p);
   for (cudaEvent_t ev : h->ev) cudaEventDestroy(ev);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   for (rgf_handle_s* w : h->workers) rgf_destroy(w);
@@ -1783,6 +1860,17 @@ rgf_status rgf_last_engine(rgf_handle h, int32_t* engine, int32_t* fallback, dou
   if (engine) *engine = h->engine_used;
   if (fallback) *fallback = h->fallback;
   if (rejected_probe) *rejected_probe = h->fallback ? h->probe_first : 0.0;
+  return RGF_OK;
+}
+
+rgf_status rgf_last_refinement(rgf_handle h, int32_t* form, int32_t* iterations, double* last_change,
+                               double* factor_ms, double* solve_ms) {
+  if (rgf_status st = check_handle(h)) return st;
+  if (form) *form = h->mx_fallback ? -RGF_TF32X3 : h->mx_form;
+  if (iterations) *iterations = h->mx_stats.iterations;
+  if (last_change) *last_change = h->mx_stats.last_change;
+  if (factor_ms) *factor_ms = h->mx_stats.factor_ms;
+  if (solve_ms) *solve_ms = h->mx_stats.solve_ms;
   return RGF_OK;
 }
 
