@@ -272,6 +272,59 @@ def grad_over_fwd(h, dev, stream, reps: int = 5):
                         "F = sum|t|^2, checkpoint every 23 slices"}
 
 
+def precision_form(step, read_S, S_fp64, h, flush, stream, fp64_value, gpath, dev, reps: int = 2):
+    """The split-precision form (RGF_TF32X3: FP32 slice factorization with
+    3xTF32 tcgen05 updates + FP64 refinement of the whole solve) on the
+    config-2 structure, timed like `value` (device-resident epsilon and S,
+    CUDA events, L2 flushed); its S against the oracle fixture and against
+    this run's FP64 S.  Config 3 (3D, N = 576, L = 300) beside it, host-timed
+    through the Python API, error against its oracle fixture."""
+    import torch
+
+    import rgf_b200
+    from rgf_b200 import _abi, workloads
+    step()  # warm-up: allocates the factor store
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(reps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    info = h.refinement()
+    Sp = read_S()
+    v = 1000.0 / statistics.median(ts)
+    out = {"value": v, "unit": UNIT, "ratio_to_fp64": v / fp64_value, "ms_per_S": statistics.median(ts),
+           "form_used": {_abi.RGF_TF32X3: "split precision (its own S)", -_abi.RGF_TF32X3: "fell back to FP64",
+                         _abi.RGF_FP64: "FP64"}.get(info["form"], info["form"]),
+           "refinement_passes": info["iterations"], "last_correction": info["last_change"],
+           "factor_ms": info["factor_ms"], "solve_ms": info["solve_ms"],
+           "rel_err_vs_fp64_this_run": float(np.linalg.norm(Sp - S_fp64) / np.linalg.norm(S_fp64)),
+           "workload": "config2 (as value)",
+           "compared_with": "the FP64 plain form of this line (persistent FP64 DMMA sweep)"}
+    if os.path.exists(gpath):
+        S0 = np.load(gpath, allow_pickle=True)["S"]
+        out["rel_err_vs_oracle"] = float(np.linalg.norm(Sp - S0) / np.linalg.norm(S0))
+    g3 = os.path.join(ROOT, "tests", "golden", "cfg3.npz")
+    syst3, out3, in3 = workloads.config3()
+    c3 = {"workload": "config3: 3D 24x24 (N=576), L=300, Bloch (0.3, 0.7), eps {1, 2.25} p=0.4, k0dx=2pi/12, full S"}
+    for name, prec in (("fp64", _abi.RGF_FP64), ("tf32x3", _abi.RGF_TF32X3)):
+        rgf_b200.cal_smatrix_RGF_3D(syst3, out3, in3, options={"precision": prec}, handle=h)
+        t0 = time.perf_counter()
+        S3, _ = rgf_b200.cal_smatrix_RGF_3D(syst3, out3, in3, options={"precision": prec}, handle=h)
+        c3[f"{name}_ms"] = (time.perf_counter() - t0) * 1e3
+        if os.path.exists(g3):
+            S30 = np.load(g3, allow_pickle=True)["S"]
+            c3[f"{name}_rel_err_vs_oracle"] = float(np.linalg.norm(S3 - S30) / np.linalg.norm(S30))
+    c3["tf32x3_form_used"] = h.refinement()["form"]
+    out["config3"] = c3
+    return out
+
+
 def batch_rate(dev, count: int = 256, workers: int = 0):
     """Config-4 batched form: all 256 seeded structures (N uniform 64..512,
     L uniform 100..2000, eps 1+2U, complex k0dx), full S each, through
@@ -397,7 +450,6 @@ def run_ours(args, dist):
     line["slices_per_s"] = value * 4096
     line["canonical_flops_per_S"] = F
     line["canonical_tflops"] = F * value / 1e12 / dist.world
-    line["precision_form"] = None
     line["grad_over_fwd"] = grad_over_fwd(h, dev, stream) if not args.slices else None
     line["batch"] = batch_rate(dev, workers=0) if not args.slices else None
     line["batch_pipelines"] = batch_rate(dev, workers=16) if not args.slices else None
@@ -429,6 +481,17 @@ def run_ours(args, dist):
     line["reciprocity_err"] = float(np.abs(S - S.T).max())
     line["slice_check"] = {"probe_residual": probe, "engine": "persistent (in-block pivoting)" if used == 0 else
                            "per-step (whole-column pivoting)", "recomputed": bool(fallback)}
+    # the split-precision form on the same structure, device-resident like `value`
+    if not args.slices:
+        def prec_step():
+            opt = _abi.Options(_abi.RGF_TF32X3, 0, 1, 0)
+            s = syst_struct(eps_dev.data_ptr(), 1)
+            _abi.check(lib.rgf_smatrix_2d(h.h, ctypes.byref(s), ctypes.byref(req), ctypes.byref(opt),
+                                          S_dev.data_ptr(), n_out, None))
+        line["precision_form"] = precision_form(prec_step, lambda: S_dev.cpu().numpy().T, S, h, flush, stream,
+                                                value, gpath, dev)
+    else:
+        line["precision_form"] = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count()
         v, per_slice, setup = cpu_oracle_rate(syst, out, in_, args.ref_slices)

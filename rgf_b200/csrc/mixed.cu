@@ -31,6 +31,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <utility>
 #include <vector>
 
 #include "mixed.cuh"
@@ -40,14 +41,14 @@
 namespace rgf {
 namespace {
 
-constexpr int NB = 64;            // pivot block width (complex)
-constexpr int KB = 2 * NB;        // real K of the update GEMM
-constexpr int kSolveBN = 64;      // tile width of the solve GEMMs
-constexpr int kUpdateBN = 128;    // tile width of the update GEMMs
+constexpr int NB = 32;            // pivot block width (complex)
 constexpr int kMaxIter = 8;
-// x has converged when the last correction, or the correction the next pass
-// would make (the last one times the observed contraction), is below this
+// x has converged when the last correction is below kTolStop, or the
+// correction the next pass would make (the last one times the observed
+// contraction) is below kTolNext -- two orders of magnitude under the 1e-10
+// the split-precision form is held to
 constexpr double kTolStop = 1e-13;
+constexpr double kTolNext = 1e-12;
 constexpr long long kGemmTimeout = 4000000000LL;  // ~2 s of SM clock
 
 #define RGF_CUDA_TRY_MX(call)                                                            \
@@ -72,6 +73,28 @@ __device__ __forceinline__ void split2(float a, float b, float* hi, float* lo) {
 __device__ __forceinline__ float2 fcmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+// programmatic dependent launch: let the next kernel of the stream start its
+// prologue, and wait for the previous one before touching its results
+__device__ __forceinline__ void pdl_open() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+// launch with programmatic stream serialization (every kernel launched this
+// way waits for its predecessor with pdl_wait before it reads or writes)
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                       Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
 
 // ---------------------------------------------------------------------------
 // factorization kernels
@@ -84,6 +107,8 @@ __device__ __forceinline__ float2 fcmul(float2 a, float2 b) {
 __global__ void k_mx_assemble(float2* W, int64_t ldw, int64_t N, float* st_hi, float* st_lo, int store,
                               int assemble, const int* st_col, const double2* st_val, double2 k2,
                               const double2* eps, const double2* Ga, const double2* Gb) {
+  pdl_open();
+  pdl_wait();
   const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (j >= ldw) return;
   for (int64_t i = blockIdx.y; i < N; i += gridDim.y) {
@@ -109,120 +134,6 @@ __global__ void k_mx_assemble(float2* W, int64_t ldw, int64_t N, float* st_hi, f
   }
 }
 
-// Block 0: T = inverse of the jn x jn pivot block W(J, J) by Gauss-Jordan on
-// diagonal pivots, register-resident (thread t holds row t/4, columns
-// t%4 + 4q), one barrier per pivot; T is NB x NB with zero padding.  Flags
-// kStatusSingular on a zero or non-finite pivot.
-// Blocks 1..: the update's left operand V = W(:, J) - E_J (E_J the identity's
-// columns J), split hi/lo, NB complex columns per row (zero beyond jn).
-__global__ void __launch_bounds__(256) k_mx_panel(const float2* W, int64_t ldw, int64_t N, int64_t j0, int jn,
-                                                  float2* T, float* V_hi, float* V_lo, int* status) {
-  const int tid = threadIdx.x;
-  if (blockIdx.x == 0) {
-    __shared__ float2 rowb[2][NB];
-    __shared__ float2 colb[2][NB];
-    const int r = tid >> 2, cq = tid & 3;
-    float2 a[16];
-#pragma unroll
-    for (int q = 0; q < 16; q++) {
-      const int c = cq + 4 * q;
-      a[q] = (r < jn && c < jn) ? W[(j0 + r) * ldw + j0 + c] : make_float2(0.f, 0.f);
-    }
-    bool bad = false;
-    for (int k = 0; k < jn; k++) {
-      const int b = k & 1;
-      if (r == k) {
-#pragma unroll
-        for (int q = 0; q < 16; q++) rowb[b][cq + 4 * q] = a[q];
-      }
-      if (cq == (k & 3)) {
-#pragma unroll
-        for (int q = 0; q < 16; q++)
-          if (q == (k >> 2)) colb[b][r] = a[q];
-      }
-      __syncthreads();
-      const float2 p = rowb[b][k];
-      const float d = p.x * p.x + p.y * p.y;
-      const float id = 1.f / d;
-      const float2 pinv = make_float2(p.x * id, -p.y * id);
-      if (!(d > 0.f) || !isfinite(id)) bad = true;
-      if (r == k) {
-#pragma unroll
-        for (int q = 0; q < 16; q++) a[q] = (cq + 4 * q == k) ? pinv : fcmul(a[q], pinv);
-      } else {
-        const float2 fp = fcmul(colb[b][r], pinv);
-#pragma unroll
-        for (int q = 0; q < 16; q++) {
-          const int c = cq + 4 * q;
-          const float2 u = fcmul(fp, rowb[b][c]);
-          a[q] = (c == k) ? make_float2(-fp.x, -fp.y) : make_float2(a[q].x - u.x, a[q].y - u.y);
-        }
-      }
-    }
-    if (bad && tid == 0) atomicOr(status, kStatusSingular);
-#pragma unroll
-    for (int q = 0; q < 16; q++) T[r * NB + cq + 4 * q] = a[q];
-    return;
-  }
-  const int64_t r0 = (int64_t)(blockIdx.x - 1) * 64;
-  for (int e = tid; e < 64 * NB; e += 256) {
-    const int64_t i = r0 + e / NB;
-    const int t = e % NB;
-    if (i >= N) break;
-    float2 w = make_float2(0.f, 0.f);
-    if (t < jn) {
-      w = W[i * ldw + j0 + t];
-      if (i == j0 + t) w.x -= 1.f;
-    }
-    split2(w.x, w.y, V_hi + i * KB + 2 * t, V_lo + i * KB + 2 * t);
-  }
-}
-
-// Row panel U = T W'(J, :) (W'(J, J) = I, so U(:, J) = T) for 16 columns per
-// block, written as the update's right operand: rows 2c, 2c+1 of Ut (K = 2t,
-// 2t+1), Ut[2c][2t] = Re U[t][c], Ut[2c][2t+1] = -Im, Ut[2c+1][2t] = Im,
-// Ut[2c+1][2t+1] = Re; hi/lo split.
-__global__ void __launch_bounds__(256) k_mx_rowpanel(const float2* W, int64_t ldw, int64_t N, int64_t j0, int jn,
-                                                     const float2* T, float* U_hi, float* U_lo) {
-  __shared__ float2 Ts[NB][NB + 1];
-  __shared__ float2 Ws[NB][17];
-  const int tid = threadIdx.x;
-  const int64_t c0 = (int64_t)blockIdx.x * 16;
-  for (int e = tid; e < NB * NB; e += 256) Ts[e / NB][e % NB] = T[e];
-  for (int e = tid; e < NB * 16; e += 256) {
-    const int sr = e / 16, cl = e % 16;
-    const int64_t c = c0 + cl;
-    float2 w = make_float2(0.f, 0.f);
-    if (c < N && sr < jn) {
-      if (c >= j0 && c < j0 + jn)
-        w.x = (j0 + sr == c) ? 1.f : 0.f;
-      else
-        w = W[(j0 + sr) * ldw + c];
-    }
-    Ws[sr][cl] = w;
-  }
-  __syncthreads();
-  const int t = tid >> 2, cl0 = (tid & 3) * 4;
-  float2 acc[4] = {};
-  for (int sr = 0; sr < NB; sr++) {
-    const float2 tv = Ts[t][sr];
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-      const float2 wv = Ws[sr][cl0 + u];
-      acc[u].x += tv.x * wv.x - tv.y * wv.y;
-      acc[u].y += tv.x * wv.y + tv.y * wv.x;
-    }
-  }
-#pragma unroll
-  for (int u = 0; u < 4; u++) {
-    const int64_t c = c0 + cl0 + u;
-    if (c >= N) break;
-    const float2 v = acc[u];
-    split2(v.x, -v.y, U_hi + (2 * c) * KB + 2 * t, U_lo + (2 * c) * KB + 2 * t);
-    split2(v.y, v.x, U_hi + (2 * c + 1) * KB + 2 * t, U_lo + (2 * c + 1) * KB + 2 * t);
-  }
-}
-
 // ---------------------------------------------------------------------------
 // refinement kernels.  Vectors are N x P row-major per slice (site, column):
 // x (FP64, L slices), y (FP32, L slices), the GEMM partials (ksplit x N x P
@@ -242,7 +153,9 @@ __device__ __forceinline__ float2 sum_parts(const float2* part, int ksplit, int6
 // write the transposed tile (tile[p][i]) as rows 2p, 2p+1 of Bt
 __device__ __forceinline__ void store_bt(float2 (&tile)[32][33], int64_t p0, int64_t i0, int64_t N, int64_t P,
                                          float* bt_hi, float* bt_lo, int64_t lda) {
-  for (int q = threadIdx.y; q < 32; q += 8) {
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    const int q = threadIdx.y + 8 * u;
     const int64_t p = p0 + q, i = i0 + threadIdx.x;
     if (p < P && i < N) {
       const float2 v = tile[q][threadIdx.x];
@@ -252,47 +165,69 @@ __device__ __forceinline__ void store_bt(float2 (&tile)[32][33], int64_t p0, int
   }
 }
 
-// forward pass, slice k: y_{k-1} = (GEMM partials) -> ystore; r_k = b_k - (H x)_k
-// in FP64; v_k = r_k + y_{k-1} -> Bt.
-__global__ void __launch_bounds__(256) k_mx_fwd_prep(int64_t k, int64_t L, int64_t N, int64_t P, const double2* x,
-                                                     float2* ystore, const float2* part, int ksplit,
-                                                     const double2* eps_k, const int* st_col,
+// residual of the whole solve in FP64, every slice at once:
+//   r_k = b_k - (H x)_k = b_k - A_k x_k + x_{k-1} + x_{k+1} (+ G0_L x_0 at k = 0,
+//   + G0_R x_{L-1} at k = L-1), stored in FP32 in r (= the y buffer: the
+// forward pass replaces r_k by y_k once r_{k+1} has been read).
+// Block: 32 columns x 8 sites of one slice (grid z = slice).
+__global__ void __launch_bounds__(256) k_mx_residual(int64_t L, int64_t N, int64_t P, const double2* x,
+                                                     float2* r, const double2* eps, const int* st_col,
                                                      const double2* st_val, double2 k2, const double2* b0,
-                                                     const double2* bL, const double2* e0, const double2* e1,
-                                                     float* bt_hi, float* bt_lo, int64_t lda) {
+                                                     const double2* bL, const double2* e0, const double2* e1) {
+  pdl_open();
+  pdl_wait();
+  const int64_t NP = N * P;
+  const int64_t p = blockIdx.x * 32 + threadIdx.x, i = blockIdx.y * 8 + threadIdx.y;
+  if (p >= P || i >= N) return;
+  const int64_t ip = i * P + p;
+  for (int64_t k = blockIdx.z; k < L; k += gridDim.z) {
+  const double2* xk = x + k * NP;
+  double2 v = cmk(0.0, 0.0);
+  if (k == 0) {
+    v = cadd(v, b0[ip]);
+    if (e0) v = cadd(v, e0[ip]);
+  }
+  if (k == L - 1) {
+    v = cadd(v, bL[ip]);
+    if (e1) v = cadd(v, e1[ip]);
+  }
+  double2 ax = cneg(cmul(cmul(k2, eps[k * N + i]), xk[ip]));
+#pragma unroll
+  for (int q = 0; q < kMaxStencil; q++) {
+    const int c = st_col[i * kMaxStencil + q];
+    if (c >= 0) ax = cadd(ax, cmul(st_val[i * kMaxStencil + q], xk[(int64_t)c * P + p]));
+  }
+  v = csub(v, ax);
+  if (k > 0) v = cadd(v, xk[ip - NP]);
+  if (k < L - 1) v = cadd(v, xk[ip + NP]);
+  r[k * NP + ip] = make_float2((float)v.x, (float)v.y);
+  }
+}
+
+// forward pass, slice k: y_{k-1} = (GEMM partials) -> ystore[k-1] (over
+// r_{k-1}); v_k = r_k + y_{k-1} -> Bt.
+__global__ void __launch_bounds__(256) k_mx_fwd_prep(int64_t k, int64_t N, int64_t P, float2* ystore,
+                                                     const float2* part, int ksplit, float* bt_hi, float* bt_lo,
+                                                     int64_t lda) {
+  pdl_open();
+  pdl_wait();
   __shared__ float2 tile[32][33];
   const int64_t p0 = blockIdx.x * 32, i0 = blockIdx.y * 32, NP = N * P;
   const int64_t p = p0 + threadIdx.x;
-  const double2* xk = x + k * NP;
-  for (int q = threadIdx.y; q < 32; q += 8) {
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    const int q = threadIdx.y + 8 * u;
     const int64_t i = i0 + q;
     float2 v = make_float2(0.f, 0.f);
     if (i < N && p < P) {
       const int64_t ip = i * P + p;
-      float2 yp = make_float2(0.f, 0.f);
+      v = ystore[k * NP + ip];  // r_k
       if (k > 0) {
-        yp = sum_parts(part, ksplit, NP, ip);
+        const float2 yp = sum_parts(part, ksplit, NP, ip);
         ystore[(k - 1) * NP + ip] = yp;
+        v.x += yp.x;
+        v.y += yp.y;
       }
-      double2 r = cmk(0.0, 0.0);
-      if (k == 0) {
-        r = cadd(r, b0[ip]);
-        if (e0) r = cadd(r, e0[ip]);
-      }
-      if (k == L - 1) {
-        r = cadd(r, bL[ip]);
-        if (e1) r = cadd(r, e1[ip]);
-      }
-      double2 ax = cneg(cmul(cmul(k2, eps_k[i]), xk[ip]));
-#pragma unroll
-      for (int qq = 0; qq < kMaxStencil; qq++) {
-        const int c = st_col[i * kMaxStencil + qq];
-        if (c >= 0) ax = cadd(ax, cmul(st_val[i * kMaxStencil + qq], xk[(int64_t)c * P + p]));
-      }
-      r = csub(r, ax);
-      if (k > 0) r = cadd(r, xk[ip - NP]);
-      if (k < L - 1) r = cadd(r, xk[ip + NP]);
-      v = make_float2((float)r.x + yp.x, (float)r.y + yp.y);
     }
     tile[threadIdx.x][q] = v;
   }
@@ -306,12 +241,16 @@ __global__ void __launch_bounds__(256) k_mx_fwd_prep(int64_t k, int64_t L, int64
 __global__ void __launch_bounds__(256) k_mx_bwd_prep(int64_t k, int64_t L, int64_t N, int64_t P, double2* x,
                                                      const float2* ystore, const float2* part, int ksplit,
                                                      float* bt_hi, float* bt_lo, int64_t lda, double* norms) {
+  pdl_open();
+  pdl_wait();
   __shared__ float2 tile[32][33];
   __shared__ double red[2][8];
   const int64_t p0 = blockIdx.x * 32, i0 = blockIdx.y * 32, NP = N * P;
   const int64_t p = p0 + threadIdx.x;
   double dd = 0.0, xx = 0.0;
-  for (int q = threadIdx.y; q < 32; q += 8) {
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    const int q = threadIdx.y + 8 * u;
     const int64_t i = i0 + q;
     float2 d = make_float2(0.f, 0.f);
     if (i < N && p < P) {
@@ -414,6 +353,357 @@ __global__ void k_mx_delta(double2* S, int64_t ldS, const int* pairs, int npairs
   if (q < npairs) S[pairs[2 * q] + (int64_t)pairs[2 * q + 1] * ldS].x -= 1.0;
 }
 
+// ---------------------------------------------------------------------------
+// One Gauss-Jordan step of the slice inverse in a single launch:
+//   W_dst = W' - V U,  V = W(:, J) - E_J,  U = T W'(J, :),  T = W(J, J)^-1,
+//   W' = W_src with the columns J replaced by those of the identity (E_J).
+// Every CTA owns a 128 x 128 real tile of W (64 complex columns) and forms
+// T itself (redundantly: the 32-pivot chain sets the step time anyway, and
+// no CTA waits for another), U for its columns straight into the swizzled
+// shared-memory operand, the 3xTF32 product on tcgen05 (TMEM accumulator)
+// and the update.  W_src and W_dst are different buffers, so a CTA that
+// finishes early never overwrites what another still reads.  256 threads.
+// ---------------------------------------------------------------------------
+namespace gjs {
+constexpr int BN = 128;                 // real columns per tile
+constexpr uint32_t CH = 16384;          // one operand K-chunk: 128 rows x 32 fp32 (128-byte rows)
+constexpr uint32_t OFF_AH = 0, OFF_AL = 2 * CH, OFF_BH = 4 * CH, OFF_BL = 6 * CH;  // 32 KB each
+constexpr uint32_t OFF_WP = 8 * CH;     // W' tile: 4 chunks [chunk][row][32 fp32], unswizzled
+constexpr uint32_t OFF_WJC = 12 * CH;   // W'(J, tile columns): 32 x 64 float2
+constexpr uint32_t OFF_T = 13 * CH;     // T: 32 x (32 + 1) float2
+constexpr uint32_t SMEM = OFF_T + NB * (NB + 1) * 8 + 1024;
+constexpr int TP = BN + 4;              // pitch of the epilogue staging tile (over the operands)
+static_assert(128 * TP * 4 <= OFF_WP, "staging tile");
+}  // namespace gjs
+
+__device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, int* status, long long timeout) {
+  if (tc32::mbar_try(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!tc32::mbar_try(bar, parity)) {
+    if (clock64() - t0 > timeout) {
+      atomicOr(status, kStatusTimeout);
+      return false;
+    }
+  }
+  return true;
+}
+
+// Development builds only (-DRGF_MX_STAMPS, never in the shipped library):
+// %globaltimer at the phase boundaries of one CTA of the step kernel.
+#ifdef RGF_MX_STAMPS
+__device__ unsigned long long g_mx_stamps[16];
+#define MX_STAMP(i)                                                                     \
+  do {                                                                                  \
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {                       \
+      unsigned long long t_;                                                            \
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_));                           \
+      g_mx_stamps[i] = t_;                                                              \
+    }                                                                                   \
+  } while (0)
+#else
+#define MX_STAMP(i) \
+  do {              \
+  } while (0)
+#endif
+
+// X = M^-1 for a 16 x 16 complex block by one warp: Gauss-Jordan on diagonal
+// pivots with lane l holding row l/2, columns (l%2) + 2q; the pivot row, the
+// multiplier and the pivot come by shuffles, so no barrier is needed.  A zero
+// or non-finite pivot sets *bad.
+__device__ __forceinline__ void inv16_warp(const float2* M, int ldm, float2* X, int ldx, int lane, int* bad) {
+  const int r = lane >> 1, h = lane & 1;
+  float2 a[8];
+#pragma unroll
+  for (int q = 0; q < 8; q++) a[q] = M[r * ldm + h + 2 * q];
+  bool badl = false;
+#pragma unroll
+  for (int k = 0; k < 16; k++) {
+    float2 rk[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      rk[q].x = __shfl_sync(0xffffffffu, a[q].x, 2 * k + h);
+      rk[q].y = __shfl_sync(0xffffffffu, a[q].y, 2 * k + h);
+    }
+    const float2 src = a[k >> 1];
+    float2 f, p;
+    f.x = __shfl_sync(0xffffffffu, src.x, 2 * r + (k & 1));
+    f.y = __shfl_sync(0xffffffffu, src.y, 2 * r + (k & 1));
+    p.x = __shfl_sync(0xffffffffu, src.x, 2 * k + (k & 1));
+    p.y = __shfl_sync(0xffffffffu, src.y, 2 * k + (k & 1));
+    const float d = p.x * p.x + p.y * p.y;
+    const float id = __frcp_rn(d);
+    if (!(d > 0.f) || !isfinite(id)) badl = true;
+    const float2 pinv = make_float2(p.x * id, -p.y * id);
+    const bool me = (r == k);
+    const float2 fp = fcmul(f, pinv);
+    const float2 coef = me ? make_float2(-pinv.x, -pinv.y) : fp;
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const float2 u = fcmul(coef, rk[q]);
+      const float2 base = me ? make_float2(0.f, 0.f) : a[q];
+      a[q] = make_float2(base.x - u.x, base.y - u.y);
+    }
+    if (h == (k & 1)) a[k >> 1] = me ? pinv : make_float2(-fp.x, -fp.y);
+  }
+#pragma unroll
+  for (int q = 0; q < 8; q++) X[r * ldx + h + 2 * q] = a[q];
+  if (badl) *bad = 1;
+}
+
+// C (16 x 16) = sign * A B (+ D), row-major with the given leading dimensions;
+// thread t of the block computes element (t / 16, t % 16)
+__device__ __forceinline__ void mm16(const float2* A, int lda_, const float2* B, int ldb, const float2* D, int ldd,
+                                     float sign, float2* C, int ldc, int t) {
+  const int i = t >> 4, j = t & 15;
+  float2 acc = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int s = 0; s < 16; s++) {
+    const float2 u = fcmul(A[i * lda_ + s], B[s * ldb + j]);
+    acc.x += u.x;
+    acc.y += u.y;
+  }
+  float2 v = make_float2(sign * acc.x, sign * acc.y);
+  if (D) {
+    v.x += D[i * ldd + j].x;
+    v.y += D[i * ldd + j].y;
+  }
+  C[i * ldc + j] = v;
+}
+
+__global__ void __launch_bounds__(256, 1)
+    k_mx_gj_step(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapW,
+                 const float* __restrict__ Wsrc, float* __restrict__ Wdst, int64_t lda, int N, int j0, int jn,
+                 int* status, long long timeout) {
+  using namespace gjs;
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t bar_ld;
+  __shared__ __align__(8) uint64_t bar_mma;
+  __shared__ uint32_t tmem_sh;
+  __shared__ int bad;
+  pdl_open();
+  MX_STAMP(0);
+  const uint32_t sb = (tc32::su32(smem_raw) + 1023u) & ~1023u;
+  uint8_t* gb = smem_raw + (sb - tc32::su32(smem_raw));
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int m0 = blockIdx.y * 128, n0 = blockIdx.x * BN;
+  if (tid == 0) {
+    tc32::mbar_init(tc32::su32(&bar_ld), 1);
+    tc32::mbar_init(tc32::su32(&bar_mma), 1);
+    bad = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc32::su32(&tmem_sh)),
+                 "r"(BN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_sh;
+  pdl_wait();
+  MX_STAMP(1);
+
+  // (1) TMA: V's rows W_src(m0.., 2 j0 .. 2 j0 + 63) swizzled for the MMA, and the W' tile
+  const uint32_t bl = tc32::su32(&bar_ld);
+  if (tid == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bl), "r"(6 * CH) : "memory");
+    for (int kc = 0; kc < 2; kc++) tc32::tma_load_3d(sb + OFF_AH + kc * CH, &mapA, 2 * j0 + 32 * kc, m0, 0, bl);
+    for (int kc = 0; kc < 4; kc++) tc32::tma_load_3d(sb + OFF_WP + kc * CH, &mapW, n0 + 32 * kc, m0, 0, bl);
+  }
+  // (2) the pivot block (thread: row tid/8, columns tid%8 + 8q) and W(J, tile columns) into registers
+  const int r = tid >> 3, cq = tid & 7;
+  float2 a[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int c = cq + 8 * q;
+    a[q] = (r < jn && c < jn) ? *reinterpret_cast<const float2*>(Wsrc + (int64_t)(j0 + r) * lda + 2 * (j0 + c))
+                              : make_float2(0.f, 0.f);
+  }
+  float4 wj[4];
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    const int e = tid + 256 * u, row = e >> 5, n = n0 + 4 * (e & 31);
+    wj[u] = (row < jn && n < lda) ? *reinterpret_cast<const float4*>(Wsrc + (int64_t)(j0 + row) * lda + n)
+                                  : make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  MX_STAMP(2);
+  // (3) T = W(J, J)^-1 by 2 x 2 blocks of 16 (A, B; C, D): X = A^-1,
+  //     S = D - C X B, Y = S^-1, T = [[X - X B T21, -X B Y], [-Y C X, Y]];
+  //     the inverses by warp 0 (shuffles only), the products by all threads.
+  //     The block is identity-padded beyond jn and T zeroed there.  The
+  //     temporaries live in the A_lo operand area, written only later.
+  float2* Ts = reinterpret_cast<float2*>(gb + OFF_T);
+  {
+    constexpr int LD = NB + 1, L16 = 17;
+    float2* Mb = reinterpret_cast<float2*>(gb + OFF_AL);
+    float2* Xs = Mb + NB * LD;
+    float2* P1 = Xs + 16 * L16;
+    float2* P2 = P1 + 16 * L16;
+    float2* Ss = P2 + 16 * L16;
+    float2* Ys = Ss + 16 * L16;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int c = cq + 8 * q;
+      Mb[r * LD + c] = (r < jn && c < jn) ? a[q] : make_float2(r == c ? 1.f : 0.f, 0.f);
+    }
+    __syncthreads();
+    if (warp == 0) inv16_warp(Mb, LD, Xs, L16, lane, &bad);
+    __syncthreads();
+    mm16(Xs, L16, Mb + 16, LD, nullptr, 0, 1.f, P1, L16, tid);           // P1 = X B
+    mm16(Mb + 16 * LD, LD, Xs, L16, nullptr, 0, 1.f, P2, L16, tid);      // P2 = C X
+    __syncthreads();
+    mm16(Mb + 16 * LD, LD, P1, L16, Mb + 16 * LD + 16, LD, -1.f, Ss, L16, tid);  // S = D - C P1
+    __syncthreads();
+    if (warp == 0) inv16_warp(Ss, L16, Ys, L16, lane, &bad);
+    __syncthreads();
+    mm16(P1, L16, Ys, L16, nullptr, 0, -1.f, Ts + 16, LD, tid);            // T12 = -P1 Y
+    mm16(Ys, L16, P2, L16, nullptr, 0, -1.f, Ts + 16 * LD, LD, tid);       // T21 = -Y P2
+    Ts[(16 + (tid >> 4)) * LD + 16 + (tid & 15)] = Ys[(tid >> 4) * L16 + (tid & 15)];  // T22 = Y
+    __syncthreads();
+    mm16(P1, L16, Ts + 16 * LD, LD, Xs, L16, -1.f, Ts, LD, tid);          // T11 = X - P1 T21
+    __syncthreads();  // the temporaries are overwritten by the operand split below
+    if (jn < NB) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int c = cq + 8 * q;
+        if (r >= jn || c >= jn) Ts[r * LD + c] = make_float2(0.f, 0.f);
+      }
+    }
+  }
+  MX_STAMP(3);
+  // W'(J, tile columns): the pivot columns replaced by the identity's
+  float2* Wj = reinterpret_cast<float2*>(gb + OFF_WJC);
+#pragma unroll
+  for (int u = 0; u < 4; u++) {
+    const int e = tid + 256 * u, row = e >> 5, l = 2 * (e & 31);
+    const int c = (n0 >> 1) + l;
+    float2 v0 = make_float2(wj[u].x, wj[u].y), v1 = make_float2(wj[u].z, wj[u].w);
+    if (c >= j0 && c < j0 + jn) v0 = make_float2((j0 + row == c && row < jn) ? 1.f : 0.f, 0.f);
+    if (c + 1 >= j0 && c + 1 < j0 + jn) v1 = make_float2((j0 + row == c + 1 && row < jn) ? 1.f : 0.f, 0.f);
+    Wj[row * 64 + l] = v0;
+    Wj[row * 64 + l + 1] = v1;
+  }
+  // (4) V = W(:, J) - E_J, split hi/lo in place over the swizzled TMA tile
+  const bool ok_ld = wait_bar(bl, 0, status, timeout);
+  MX_STAMP(4);
+#pragma unroll
+  for (int u = 0; u < 8; u++) {
+    const int g = tid + 256 * u, kc = g >> 10, gi = g & 1023, row = gi >> 3, gp = gi & 7;
+    const int kf = kc * 32 + ((gp ^ (row & 7)) << 2);  // logical fp32 column of the granule
+    const uint32_t off = OFF_AH + kc * CH + row * 128 + gp * 16;
+    float4 x = *reinterpret_cast<const float4*>(gb + off);
+    const int m = m0 + row, t = kf >> 1;
+    if (t < jn && m == j0 + t) x.x -= 1.f;
+    if (t + 1 < jn && m == j0 + t + 1) x.z -= 1.f;
+    const float4 h = make_float4(tf32_hi(x.x), tf32_hi(x.y), tf32_hi(x.z), tf32_hi(x.w));
+    *reinterpret_cast<float4*>(gb + off) = h;
+    *reinterpret_cast<float4*>(gb + off + (OFF_AL - OFF_AH)) = make_float4(x.x - h.x, x.y - h.y, x.z - h.z, x.w - h.w);
+  }
+  __syncthreads();
+  MX_STAMP(5);
+  // (5) U = T W'(J, tile columns): lane = row t of U, warp = 8 complex columns; written as
+  //     the MMA's right operand (rows 2l, 2l+1; K = 2t, 2t+1), 128-byte swizzle, hi/lo
+  {
+    float2 acc[8];
+#pragma unroll
+    for (int v = 0; v < 8; v++) acc[v] = make_float2(0.f, 0.f);
+#pragma unroll 4
+    for (int sr = 0; sr < NB; sr++) {
+      const float2 tv = Ts[lane * (NB + 1) + sr];
+#pragma unroll
+      for (int v = 0; v < 8; v++) {
+        const float2 w = Wj[sr * 64 + warp * 8 + v];
+        acc[v].x += tv.x * w.x - tv.y * w.y;
+        acc[v].y += tv.x * w.y + tv.y * w.x;
+      }
+    }
+    const int kf = 2 * lane, kc = kf >> 5, kk = kf & 31, gq = kk >> 2, ofs = (kk & 3) * 4;
+#pragma unroll
+    for (int v = 0; v < 8; v++) {
+      const int l = warp * 8 + v;
+#pragma unroll
+      for (int hh = 0; hh < 2; hh++) {
+        const int n = 2 * l + hh;
+        const float x0 = hh ? acc[v].y : acc[v].x, x1 = hh ? acc[v].x : -acc[v].y;
+        const uint32_t off = kc * CH + n * 128 + ((gq ^ (n & 7)) << 4) + ofs;
+        const float h0 = tf32_hi(x0), h1 = tf32_hi(x1);
+        *reinterpret_cast<float2*>(gb + OFF_BH + off) = make_float2(h0, h1);
+        *reinterpret_cast<float2*>(gb + OFF_BL + off) = make_float2(x0 - h0, x1 - h1);
+      }
+    }
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // operand writes -> tensor core
+  __syncthreads();
+  MX_STAMP(6);
+  // (6) 2 K-chunks x 4 K-steps x 3 products on tcgen05
+  const uint32_t bm = tc32::su32(&bar_mma);
+  if (tid == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+    for (int kc = 0; kc < 2; kc++) {
+      const uint64_t ah = tc32::sw128_desc(sb + OFF_AH + kc * CH), al = tc32::sw128_desc(sb + OFF_AL + kc * CH);
+      const uint64_t bh = tc32::sw128_desc(sb + OFF_BH + kc * CH), blo = tc32::sw128_desc(sb + OFF_BL + kc * CH);
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) {
+        const uint64_t o = (uint64_t)(kk * 2);
+        tc32::mma_tf32(tmem, al + o, bh + o, tc32::Cfg<BN>::IDESC, (kc | kk) != 0);
+        tc32::mma_tf32(tmem, ah + o, blo + o, tc32::Cfg<BN>::IDESC, 1);
+        tc32::mma_tf32(tmem, ah + o, bh + o, tc32::Cfg<BN>::IDESC, 1);
+      }
+    }
+    tc32::mma_commit(bm);
+  }
+  __syncwarp();
+  const bool ok = wait_bar(bm, 0, status, timeout) && ok_ld;
+  MX_STAMP(7);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  // (7) epilogue: D (TMEM) -> staging over the operands -> W_dst = W' - D, one warp per row
+  float* stg = reinterpret_cast<float*>(gb + OFF_AH);
+  if (warp < 4) {
+    const int row = warp * 32 + lane;
+#pragma unroll 1
+    for (int c = 0; c < BN; c += 16) {
+      float v[16];
+      tc32::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+      float4* t4 = reinterpret_cast<float4*>(stg + row * TP + c);
+#pragma unroll
+      for (int j = 0; j < 4; j++) t4[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+    }
+  }
+  __syncthreads();
+  MX_STAMP(8);
+  if (ok) {
+    const int cc = lane * 4, n = n0 + cc;
+    const float* wp = reinterpret_cast<const float*>(gb + OFF_WP) + (cc >> 5) * (CH / 4) + (cc & 31);
+#pragma unroll 4
+    for (int rr = warp; rr < 128; rr += 8) {
+      const int m = m0 + rr;
+      if (m >= N || n >= lda) continue;
+      const float4 d = *reinterpret_cast<const float4*>(stg + rr * TP + cc);
+      float4 w = *reinterpret_cast<const float4*>(wp + rr * 32);
+      const int c0 = n >> 1;  // complex columns c0, c0 + 1
+      if (c0 >= j0 && c0 < j0 + jn) {
+        w.x = (c0 == m) ? 1.f : 0.f;
+        w.y = 0.f;
+      }
+      if (c0 + 1 >= j0 && c0 + 1 < j0 + jn) {
+        w.z = (c0 + 1 == m) ? 1.f : 0.f;
+        w.w = 0.f;
+      }
+      *reinterpret_cast<float4*>(Wdst + (int64_t)m * lda + n) = make_float4(w.x - d.x, w.y - d.y, w.z - d.z, w.w - d.w);
+    }
+  }
+  MX_STAMP(9);
+  if (bad && tid == 0 && blockIdx.x == 0 && blockIdx.y == 0) atomicOr(status, kStatusSingular);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
+}
+
 inline int64_t lda_of(int64_t N) { return (2 * N + 31) / 32 * 32; }
 
 template <int BN>
@@ -441,13 +731,16 @@ int choose_ksplit(int64_t tiles, int64_t kchunks, int sms) {
 
 }  // namespace
 
+#ifdef RGF_MX_STAMPS
+extern "C" __attribute__((visibility("default"))) int rgf_dev_mx_stamps(unsigned long long* out) {
+  return (int)cudaMemcpyFromSymbol(out, g_mx_stamps, sizeof(g_mx_stamps));
+}
+#endif
+
 size_t mixed_workspace_bytes(int64_t N, int64_t L, int64_t P) {
   const int64_t lda = lda_of(N), ldw = lda / 2;
   size_t b = 0;
-  b += sizeof(float2) * N * ldw;              // W
-  b += 2 * sizeof(float) * N * KB;            // V hi/lo
-  b += 2 * sizeof(float) * 2 * N * KB;        // U hi/lo
-  b += sizeof(float2) * NB * NB;              // T
+  b += 2 * sizeof(float2) * N * ldw;          // W, two buffers
   b += 2 * sizeof(float) * N * lda * L;       // factor store hi/lo
   b += sizeof(double2) * N * P * L;           // x
   b += sizeof(float2) * N * P * L;            // y
@@ -465,14 +758,20 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if ((st = gemm_attr<kSolveBN>()) || (st = gemm_attr<kUpdateBN>())) return st;
-  void *pW, *pV, *pU, *pT, *pSh, *pSl, *pX, *pY, *pPart, *pBt, *pVec, *pNorm, *pStat;
+  // solve GEMM tile width: the narrowest of 64 / 128 / 256 real columns that
+  // covers the request in one or two tiles keeps the factor's re-reads low
+  const int sbn = (2 * P <= 64) ? 64 : (2 * P <= 128) ? 128 : 256;
+  if ((st = gemm_attr<64>()) || (st = gemm_attr<128>()) || (st = gemm_attr<256>())) return st;
+  if (cudaFuncSetAttribute(k_mx_gj_step, cudaFuncAttributeMaxDynamicSharedMemorySize, gjs::SMEM) != cudaSuccess) {
+    set_error("cannot configure the Gauss-Jordan step kernel's shared memory");
+    return RGF_ERR_CUDA;
+  }
+  void *pW, *pSh, *pSl, *pX, *pY, *pPart, *pBt, *pVec, *pNorm, *pStat;
   const int ntile_m = (int)((N + tc32::BM - 1) / tc32::BM);
-  const int ntile_s = (int)((2 * P + kSolveBN - 1) / kSolveBN);
+  const int ntile_s = (int)((2 * P + sbn - 1) / sbn);
   const int kchunks = (int)(lda / tc32::BK);
   const int ksplit = choose_ksplit((int64_t)ntile_m * ntile_s, kchunks, sms);
-  if ((st = alloc(kMxW, sizeof(float2) * N * ldw, &pW)) || (st = alloc(kMxV, 2 * sizeof(float) * N * KB, &pV)) ||
-      (st = alloc(kMxU, 2 * sizeof(float) * 2 * N * KB, &pU)) || (st = alloc(kMxT, sizeof(float2) * NB * NB, &pT)) ||
+  if ((st = alloc(kMxW, 2 * sizeof(float) * N * lda, &pW)) ||
       (st = alloc(kMxStoreHi, sizeof(float) * N * lda * L, &pSh)) ||
       (st = alloc(kMxStoreLo, sizeof(float) * N * lda * L, &pSl)) ||
       (st = alloc(kMxX, sizeof(double2) * NP * L, &pX)) || (st = alloc(kMxY, sizeof(float2) * NP * L, &pY)) ||
@@ -481,12 +780,7 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
       (st = alloc(kMxVec, sizeof(double2) * NP * 6, &pVec)) || (st = alloc(kMxNorm, sizeof(double) * 8, &pNorm)) ||
       (st = alloc(kMxStatus, sizeof(int), &pStat)))
     return st;
-  float2* W = static_cast<float2*>(pW);
-  float* V_hi = static_cast<float*>(pV);
-  float* V_lo = V_hi + N * KB;
-  float* U_hi = static_cast<float*>(pU);
-  float* U_lo = U_hi + 2 * N * KB;
-  float2* T = static_cast<float2*>(pT);
+  float* Wb[2] = {static_cast<float*>(pW), static_cast<float*>(pW) + N * lda};
   float* st_hi = static_cast<float*>(pSh);
   float* st_lo = static_cast<float*>(pSl);
   double2* x = static_cast<double2*>(pX);
@@ -503,20 +797,23 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
   double* norms = static_cast<double*>(pNorm);
   int* mstat = static_cast<int*>(pStat);
 
-  // tensor maps: update operands (V: N rows, Ut: 2N rows, K = 128), factor
-  // store (N rows x lda, L slices), solve right operand (2P rows x lda)
-  CUtensorMap mVh, mVl, mUh, mUl, mSh, mSl, mBh, mBl;
-  if (!(tc32::make_map(&mVh, V_hi, KB, N, 1, KB, 0, tc32::BM) && tc32::make_map(&mVl, V_lo, KB, N, 1, KB, 0, tc32::BM) &&
-        tc32::make_map(&mUh, U_hi, KB, 2 * N, 1, KB, 0, kUpdateBN) &&
-        tc32::make_map(&mUl, U_lo, KB, 2 * N, 1, KB, 0, kUpdateBN) &&
+  // tensor maps: the two W buffers (swizzled 32-column boxes for the update's
+  // left operand, unswizzled ones for the W' tile), the factor store (N rows x
+  // lda, L slices) and the solve's right operand (2P rows x lda)
+  CUtensorMap mA[2], mWp[2], mSh, mSl, mBh, mBl;
+  if (!(tc32::make_map(&mA[0], Wb[0], lda, N, 1, lda, 0, tc32::BM) &&
+        tc32::make_map(&mA[1], Wb[1], lda, N, 1, lda, 0, tc32::BM) &&
+        tc32::make_map(&mWp[0], Wb[0], lda, N, 1, lda, 0, tc32::BM, CU_TENSOR_MAP_SWIZZLE_NONE) &&
+        tc32::make_map(&mWp[1], Wb[1], lda, N, 1, lda, 0, tc32::BM, CU_TENSOR_MAP_SWIZZLE_NONE) &&
         tc32::make_map(&mSh, st_hi, lda, N, L, lda, N * lda, tc32::BM) &&
         tc32::make_map(&mSl, st_lo, lda, N, L, lda, N * lda, tc32::BM) &&
-        tc32::make_map(&mBh, bt_hi, lda, 2 * P, 1, lda, 0, kSolveBN) &&
-        tc32::make_map(&mBl, bt_lo, lda, 2 * P, 1, lda, 0, kSolveBN))) {
+        tc32::make_map(&mBh, bt_hi, lda, 2 * P, 1, lda, 0, sbn) &&
+        tc32::make_map(&mBl, bt_lo, lda, 2 * P, 1, lda, 0, sbn))) {
     set_error("tensor-map encoding for the tcgen05 GEMM failed");
     return RGF_ERR_CUDA;
   }
   RGF_CUDA_TRY_MX(cudaMemsetAsync(mstat, 0, sizeof(int), s));
+  RGF_CUDA_TRY_MX(cudaMemsetAsync(Wb[0], 0, 2 * sizeof(float) * N * lda, s));
   RGF_CUDA_TRY_MX(cudaMemsetAsync(bt_hi, 0, 2 * sizeof(float) * 2 * P * lda, s));
   RGF_CUDA_TRY_MX(cudaMemsetAsync(x, 0, sizeof(double2) * NP * L, s));
   cudaEvent_t ev[3];
@@ -532,39 +829,27 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
   // (1) low-precision factorization
   RGF_CUDA_TRY_MX(cudaEventRecord(ev[0], s));
   const dim3 ga((unsigned)((ldw + 255) / 256), (unsigned)std::min<int64_t>(N, 8192));
-  const unsigned panel_blocks = (unsigned)(1 + (N + 63) / 64);
-  const unsigned row_blocks = (unsigned)((N + 15) / 16);
-  const dim3 gu((unsigned)((2 * N + kUpdateBN - 1) / kUpdateBN), (unsigned)ntile_m, 1);
-  tc32::GemmArgs gu_args{};
-  gu_args.M = (int)N;
-  gu_args.Nr = (int)(2 * N);
-  gu_args.k_chunks = KB / tc32::BK;
-  gu_args.mode = tc32::kGJ;
-  gu_args.out = reinterpret_cast<float*>(W);
-  gu_args.ldo = 2 * ldw;
-  gu_args.err = mstat;
-  gu_args.timeout = kGemmTimeout;
+  const dim3 ggj((unsigned)((lda + gjs::BN - 1) / gjs::BN), (unsigned)ntile_m);
+  int cur = 0;  // W buffer holding the current matrix
   for (int64_t k = 0; k < L; k++) {
     const double2* Ga = (k == 0) ? mp.G0[0] : nullptr;
     const double2* Gb = (k == L - 1) ? mp.G0[1] : nullptr;
     float* sh = k > 0 ? st_hi + (k - 1) * N * lda : st_hi;
     float* sl = k > 0 ? st_lo + (k - 1) * N * lda : st_lo;
-    k_mx_assemble<<<ga, 256, 0, s>>>(W, ldw, N, sh, sl, k > 0, 1, mp.st_col, mp.st_val, mp.k2, mp.eps + k * N, Ga,
-                                     Gb);
+    launch_pdl(k_mx_assemble, ga, dim3(256), 0, s, reinterpret_cast<float2*>(Wb[cur]), ldw, N, sh, sl, (int)(k > 0),
+               1, mp.st_col, mp.st_val, mp.k2, mp.eps + k * N, Ga, Gb);
     nl++;
     for (int64_t j0 = 0; j0 < N; j0 += NB) {
       const int jn = (int)std::min<int64_t>(NB, N - j0);
-      k_mx_panel<<<panel_blocks, 256, 0, s>>>(W, ldw, N, j0, jn, T, V_hi, V_lo, mstat);
-      k_mx_rowpanel<<<row_blocks, 256, 0, s>>>(W, ldw, N, j0, jn, T, U_hi, U_lo);
-      gu_args.gj_c0 = (int)j0;
-      gu_args.gj_nb = jn;
-      tc32::k_tc32_gemm<kUpdateBN><<<gu, tc32::kThreads, tc32::Cfg<kUpdateBN>::SMEM, s>>>(mVh, mVl, mUh, mUl,
-                                                                                           gu_args);
-      nl += 3;
+      launch_pdl(k_mx_gj_step, ggj, dim3(256), gjs::SMEM, s, mA[cur], mWp[cur], (const float*)Wb[cur],
+                 Wb[cur ^ 1], lda, (int)N, (int)j0, jn, mstat, kGemmTimeout);
+      cur ^= 1;
+      nl++;
     }
   }
-  k_mx_assemble<<<ga, 256, 0, s>>>(W, ldw, N, st_hi + (L - 1) * N * lda, st_lo + (L - 1) * N * lda, 1, 0,
-                                   mp.st_col, mp.st_val, mp.k2, mp.eps, nullptr, nullptr);
+  launch_pdl(k_mx_assemble, ga, dim3(256), 0, s, reinterpret_cast<float2*>(Wb[cur]), ldw, N,
+             st_hi + (L - 1) * N * lda, st_lo + (L - 1) * N * lda, 1, 0, mp.st_col, mp.st_val, mp.k2, mp.eps,
+             (const double2*)nullptr, (const double2*)nullptr);
   nl++;
   RGF_CUDA_TRY_MX(cudaGetLastError());
   RGF_CUDA_TRY_MX(cudaEventRecord(ev[1], s));
@@ -593,7 +878,12 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
   const dim3 tp(32, 8);
   auto gemm = [&](int64_t k) {
     gs.a_z = (int)k;
-    tc32::k_tc32_gemm<kSolveBN><<<gsg, tc32::kThreads, tc32::Cfg<kSolveBN>::SMEM, s>>>(mSh, mSl, mBh, mBl, gs);
+    if (sbn == 64)
+      launch_pdl(tc32::k_tc32_gemm<64>, gsg, dim3(tc32::kThreads), tc32::Cfg<64>::SMEM, s, mSh, mSl, mBh, mBl, gs);
+    else if (sbn == 128)
+      launch_pdl(tc32::k_tc32_gemm<128>, gsg, dim3(tc32::kThreads), tc32::Cfg<128>::SMEM, s, mSh, mSl, mBh, mBl, gs);
+    else
+      launch_pdl(tc32::k_tc32_gemm<256>, gsg, dim3(tc32::kThreads), tc32::Cfg<256>::SMEM, s, mSh, mSl, mBh, mBl, gs);
   };
   double prev = 1.0, change = 1.0;
   bool conv = false;
@@ -606,14 +896,19 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
       nl += 2;
     }
     RGF_CUDA_TRY_MX(cudaMemsetAsync(norms, 0, sizeof(double) * 8, s));
+    launch_pdl(k_mx_residual, dim3((unsigned)((P + 31) / 32), (unsigned)((N + 7) / 8), (unsigned)std::min<int64_t>(L, 65535)),
+               dim3(32, 8), 0, s, L, N, P, (const double2*)x, y, mp.eps, mp.st_col, mp.st_val, mp.k2,
+               (const double2*)b0, (const double2*)bL, (const double2*)(have_x ? e0 : nullptr),
+               (const double2*)(have_x ? e1 : nullptr));
+    nl++;
     for (int64_t k = 0; k < L; k++) {
-      k_mx_fwd_prep<<<gp, tp, 0, s>>>(k, L, N, P, x, y, part, ksplit, mp.eps + k * N, mp.st_col, mp.st_val, mp.k2,
-                                      b0, bL, have_x ? e0 : nullptr, have_x ? e1 : nullptr, bt_hi, bt_lo, lda);
+      launch_pdl(k_mx_fwd_prep, gp, tp, 0, s, k, N, P, y, (const float2*)part, ksplit, bt_hi, bt_lo, lda);
       gemm(k);
       nl += 2;
     }
     for (int64_t k = L - 1; k >= 0; k--) {
-      k_mx_bwd_prep<<<gp, tp, 0, s>>>(k, L, N, P, x, y, part, ksplit, bt_hi, bt_lo, lda, norms);
+      launch_pdl(k_mx_bwd_prep, gp, tp, 0, s, k, L, N, P, x, (const float2*)y, (const float2*)part, ksplit, bt_hi,
+                 bt_lo, lda, norms);
       nl++;
       if (k > 0) {
         gemm(k - 1);
@@ -635,7 +930,7 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
     if (!isfinite(change) || (hs & kStatusSingular)) break;
     if (it > 0) {
       const double rho = change / prev;  // observed contraction of the refinement
-      if (change <= kTolStop || (rho < 0.5 && change * rho <= kTolStop)) {
+      if (change <= kTolStop || (rho < 0.5 && change * rho <= kTolNext)) {
         conv = true;
         it++;
         break;

@@ -165,6 +165,9 @@ __global__ void __launch_bounds__(kThreads, 1)
   __shared__ uint32_t tmem_sh;
   __shared__ int abort_sh;
 
+  // programmatic dependent launch: the next kernel in the stream may start its
+  // prologue now; it waits (griddepcontrol.wait) for this grid before reading
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const uint32_t base = (su32(smem_raw) + 1023u) & ~1023u;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
@@ -194,6 +197,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_sh;
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // the operands and `out` of the grid before
 
   if (warp == 0 && lane == 0) {
     // producer: one stage = A_hi, A_lo (BM rows) and B_hi, B_lo (BN rows) of BK floats
@@ -236,40 +240,63 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
   __syncwarp();
 
-  // epilogue: thread (warp, lane) owns tile row 32*warp + lane
+  // epilogue: TMEM -> shared-memory tile (the drained pipeline buffers; thread
+  // (warp, lane) moves tile row 32*warp + lane) -> global, one warp per row so
+  // that every access is a contiguous 512-byte run
   const bool ok = mbar_wait(su32(&done_bar), 0, g);
   __syncwarp();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const int m = m0 + warp * 32 + lane;
-  if (ok && g.k_chunks > 0) {
-    float* orow = g.out + (g.mode == kPartial ? (int64_t)blockIdx.z * g.split_stride : 0) + (int64_t)m * g.ldo;
+  constexpr int TP = BN + 4;  // tile pitch in floats (row shift of 4 banks: conflict-free float4 stores)
+  static_assert(BM * TP * 4 <= S * C::STAGE_BYTES, "epilogue tile");
+  float* tile = reinterpret_cast<float*>(smem_raw + (base - su32(smem_raw)));
+  const bool run = ok && g.k_chunks > 0;
+  if (run) {
+    const int row = warp * 32 + lane;
 #pragma unroll 1
     for (int c = 0; c < BN; c += 16) {
       float v[16];
       tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
-      if (m >= g.M) continue;
-      const int nb = n0 + c;
-      if (g.mode == kGJ) {
+      float4* t4 = reinterpret_cast<float4*>(tile + row * TP + c);
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
-          const int n = nb + j;
-          if (n >= g.Nr) break;
-          const int cc = n >> 1;
-          float w;
-          if (cc >= g.gj_c0 && cc < g.gj_c0 + g.gj_nb)
-            w = ((n & 1) == 0 && cc == m) ? 1.f : 0.f;
-          else
-            w = orow[n];
-          orow[n] = w - v[j];
+      for (int j = 0; j < 4; j++) t4[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+    }
+  }
+  __syncthreads();
+  if (run) {
+    float* obase = g.out + (g.mode == kPartial ? (int64_t)blockIdx.z * g.split_stride : 0);
+    const int jlo = 2 * g.gj_c0, jhi = 2 * (g.gj_c0 + g.gj_nb);  // real columns of the pivot block
+#pragma unroll 2
+    for (int r = warp; r < BM; r += 4) {
+      const int m = m0 + r;
+      if (m >= g.M) break;
+      float* orow = obase + (int64_t)m * g.ldo;
+      for (int cc = lane * 4; cc < BN; cc += 128) {
+        const int n = n0 + cc;
+        if (n >= g.Nr) break;
+        const float4 d4 = *reinterpret_cast<const float4*>(tile + r * TP + cc);
+        const float d[4] = {d4.x, d4.y, d4.z, d4.w};
+        const bool vec = (n + 4 <= g.Nr) && ((reinterpret_cast<uintptr_t>(orow + n) & 15) == 0);
+        if (g.mode == kGJ) {
+          const bool plain = n + 4 <= jlo || n >= jhi;  // no pivot-block column among the four
+          if (vec && plain) {
+            float4 w = *reinterpret_cast<const float4*>(orow + n);
+            *reinterpret_cast<float4*>(orow + n) = make_float4(w.x - d[0], w.y - d[1], w.z - d[2], w.w - d[3]);
+          } else {
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+              const int nn = n + j;
+              if (nn >= g.Nr) break;
+              const float w = (nn >= jlo && nn < jhi) ? (((nn & 1) == 0 && (nn >> 1) == m) ? 1.f : 0.f) : orow[nn];
+              orow[nn] = w - d[j];
+            }
+          }
+        } else if (vec) {
+          *reinterpret_cast<float4*>(orow + n) = d4;
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (n + j < g.Nr) orow[n + j] = d[j];
         }
-      } else if (nb + 16 <= g.Nr && ((g.ldo & 3) == 0)) {
-        float4* o4 = reinterpret_cast<float4*>(orow + nb);
-#pragma unroll
-        for (int j = 0; j < 4; j++) o4[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
-      } else {
-#pragma unroll
-        for (int j = 0; j < 16; j++)
-          if (nb + j < g.Nr) orow[nb + j] = v[j];
       }
     }
   }
@@ -303,7 +330,8 @@ inline PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 // (floats).  ld and batch_stride must be multiples of 4 floats (16 bytes), base
 // 16-byte aligned, kdim a multiple of BK.  Returns false if the map is refused.
 inline bool make_map(CUtensorMap* map, const float* base, int64_t kdim, int64_t rows, int64_t batch, int64_t ld,
-                     int64_t batch_stride, int box_rows) {
+                     int64_t batch_stride, int box_rows,
+                     CUtensorMapSwizzle swizzle = CU_TENSOR_MAP_SWIZZLE_128B) {
   PFN_cuTensorMapEncodeTiled_v12000 fn = encode_fn();
   if (!fn || kdim % BK || ld % 4 || batch_stride % 4 || (reinterpret_cast<uintptr_t>(base) & 15) || rows < 1 ||
       batch < 1 || box_rows < 1 || box_rows > 256)
@@ -313,7 +341,7 @@ inline bool make_map(CUtensorMap* map, const float* base, int64_t kdim, int64_t 
   cuuint32_t box[3] = {(cuuint32_t)BK, (cuuint32_t)box_rows, 1};
   cuuint32_t es[3] = {1, 1, 1};
   CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, es,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
