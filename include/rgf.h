@@ -328,9 +328,9 @@ RGF_API rgf_status rgf_set_stream(rgf_handle h, void* stream);
  * which puts the largest ny near 615 for the full S of a periodic problem at
  * k0dx = 2 pi / 15 (about 2 ny / 15 channels per side).  Work is issued on
  * `stream` (a cudaStream_t; NULL = the legacy default stream) of the current
- * device.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture.  Every call on a device shares the one array,
+ * device.  Every call looks up the array's device address on the current
+ * device (cudaGetSymbolAddress, which allocates nothing), so a context that
+ * the host application reset is followed.  Every call on a device shares the one array,
  * so calls that overlap on the GPU (other host threads, other streams) race;
  * each call clears what must start at zero.  opt->profile must be 0. */
 #define RGF_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)

@@ -45,10 +45,11 @@ constexpr int NB = 32;            // pivot block width (complex)
 constexpr int kMaxIter = 8;
 // x has converged when the last correction is below kTolStop, or the
 // correction the next pass would make (the last one times the observed
-// contraction) is below kTolNext -- two orders of magnitude under the 1e-10
-// the split-precision form is held to
+// contraction, measured over the whole solution and over its first and last
+// slices, which S is formed from) is below kTolNext -- an order of magnitude
+// under the 1e-10 the split-precision form is held to
 constexpr double kTolStop = 1e-13;
-constexpr double kTolNext = 1e-12;
+constexpr double kTolNext = 1e-11;
 constexpr long long kGemmTimeout = 4000000000LL;  // ~2 s of SM clock
 
 #define RGF_CUDA_TRY_MX(call)                                                            \
@@ -206,13 +207,13 @@ __global__ void __launch_bounds__(256) k_mx_residual(int64_t L, int64_t N, int64
 
 // forward pass, slice k: y_{k-1} = (GEMM partials) -> ystore[k-1] (over
 // r_{k-1}); v_k = r_k + y_{k-1} -> Bt.
-__global__ void __launch_bounds__(256) k_mx_fwd_prep(int64_t k, int64_t N, int64_t P, float2* ystore,
-                                                     const float2* part, int ksplit, float* bt_hi, float* bt_lo,
-                                                     int64_t lda) {
+__global__ void __launch_bounds__(256) k_mx_fwd_prep(int64_t k, int64_t N, int64_t P, int64_t ldp, int64_t poff,
+                                                     float2* ystore, const float2* part, int ksplit, float* bt_hi,
+                                                     float* bt_lo, int64_t lda) {
   pdl_open();
   pdl_wait();
   __shared__ float2 tile[32][33];
-  const int64_t p0 = blockIdx.x * 32, i0 = blockIdx.y * 32, NP = N * P;
+  const int64_t p0 = blockIdx.x * 32, i0 = blockIdx.y * 32, NP = N * ldp;
   const int64_t p = p0 + threadIdx.x;
 #pragma unroll
   for (int u = 0; u < 4; u++) {
@@ -220,10 +221,10 @@ __global__ void __launch_bounds__(256) k_mx_fwd_prep(int64_t k, int64_t N, int64
     const int64_t i = i0 + q;
     float2 v = make_float2(0.f, 0.f);
     if (i < N && p < P) {
-      const int64_t ip = i * P + p;
+      const int64_t ip = i * ldp + poff + p;
       v = ystore[k * NP + ip];  // r_k
       if (k > 0) {
-        const float2 yp = sum_parts(part, ksplit, NP, ip);
+        const float2 yp = sum_parts(part, ksplit, N * P, i * P + p);
         ystore[(k - 1) * NP + ip] = yp;
         v.x += yp.x;
         v.y += yp.y;
@@ -238,14 +239,15 @@ __global__ void __launch_bounds__(256) k_mx_fwd_prep(int64_t k, int64_t N, int64
 // backward pass, slice k: d_k = y_k + (GEMM partials) (k = L-1: the partials
 // are y_{L-1}); x_k += d_k in FP64; norms of d and x (whole; slice 0; slice
 // L-1); for k > 0 d_k -> Bt.
-__global__ void __launch_bounds__(256) k_mx_bwd_prep(int64_t k, int64_t L, int64_t N, int64_t P, double2* x,
+__global__ void __launch_bounds__(256) k_mx_bwd_prep(int64_t k, int64_t L, int64_t N, int64_t P, int64_t ldp,
+                                                     int64_t poff, double2* x,
                                                      const float2* ystore, const float2* part, int ksplit,
                                                      float* bt_hi, float* bt_lo, int64_t lda, double* norms) {
   pdl_open();
   pdl_wait();
   __shared__ float2 tile[32][33];
   __shared__ double red[2][8];
-  const int64_t p0 = blockIdx.x * 32, i0 = blockIdx.y * 32, NP = N * P;
+  const int64_t p0 = blockIdx.x * 32, i0 = blockIdx.y * 32, NP = N * ldp;
   const int64_t p = p0 + threadIdx.x;
   double dd = 0.0, xx = 0.0;
 #pragma unroll
@@ -254,8 +256,8 @@ __global__ void __launch_bounds__(256) k_mx_bwd_prep(int64_t k, int64_t L, int64
     const int64_t i = i0 + q;
     float2 d = make_float2(0.f, 0.f);
     if (i < N && p < P) {
-      const int64_t ip = i * P + p;
-      d = sum_parts(part, ksplit, NP, ip);
+      const int64_t ip = i * ldp + poff + p;
+      d = sum_parts(part, ksplit, N * P, i * P + p);
       if (k < L - 1) {
         const float2 y = ystore[k * NP + ip];
         d.x += y.x;
@@ -431,7 +433,8 @@ __device__ __forceinline__ void inv16_warp(const float2* M, int ldm, float2* X, 
     p.x = __shfl_sync(0xffffffffu, src.x, 2 * k + (k & 1));
     p.y = __shfl_sync(0xffffffffu, src.y, 2 * k + (k & 1));
     const float d = p.x * p.x + p.y * p.y;
-    const float id = __frcp_rn(d);
+    float id;  // approximate reciprocal (one instruction): the factor only preconditions the refinement
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(id) : "f"(d));
     if (!(d > 0.f) || !isfinite(id)) badl = true;
     const float2 pinv = make_float2(p.x * id, -p.y * id);
     const bool me = (r == k);
@@ -470,10 +473,161 @@ __device__ __forceinline__ void mm16(const float2* A, int lda_, const float2* B,
   C[i * ldc + j] = v;
 }
 
+// C (32 x 32) = sign * A B (+ D) in shared memory (leading dimension 33) by
+// 256 threads: thread t computes row t/8, columns t%8 + 8q
+__device__ __forceinline__ void mm32(const float2* A, const float2* B, const float2* D, float sign, float2* C,
+                                     int t) {
+  constexpr int LD = NB + 1;
+  const int i = t >> 3, c0 = t & 7;
+  float2 acc[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) acc[q] = make_float2(0.f, 0.f);
+#pragma unroll 8
+  for (int s = 0; s < NB; s++) {
+    const float2 av = A[i * LD + s];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const float2 u = fcmul(av, B[s * LD + c0 + 8 * q]);
+      acc[q].x += u.x;
+      acc[q].y += u.y;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    float2 v = make_float2(sign * acc[q].x, sign * acc[q].y);
+    if (D) {
+      v.x += D[i * LD + c0 + 8 * q].x;
+      v.y += D[i * LD + c0 + 8 * q].y;
+    }
+    C[i * LD + c0 + 8 * q] = v;
+  }
+}
+
+// T = M^-1 for the identity-padded 32 x 32 pivot block M (shared memory,
+// leading dimension 33) by 2 x 2 blocks of 16 (A, B; C, D): X = A^-1,
+// S = D - C X B, Y = S^-1, T = [[X - X B T21, -X B Y], [-Y C X, Y]]; the two
+// 16 x 16 inverses by warp 0 (shuffles only), the products by all 256
+// threads.  tmp: 5 x 16 x 17 float2 of shared memory.  T is zeroed beyond jn.
+__device__ __forceinline__ void inv32_block(const float2* Mb, float2* Ts, float2* tmp, int jn, int tid, int* bad) {
+  constexpr int LD = NB + 1, L16 = 17;
+  const int warp = tid >> 5, lane = tid & 31;
+  float2* Xs = tmp;
+  float2* P1 = Xs + 16 * L16;
+  float2* P2 = P1 + 16 * L16;
+  float2* Ss = P2 + 16 * L16;
+  float2* Ys = Ss + 16 * L16;
+  if (warp == 0) inv16_warp(Mb, LD, Xs, L16, lane, bad);
+  __syncthreads();
+  mm16(Xs, L16, Mb + 16, LD, nullptr, 0, 1.f, P1, L16, tid);           // P1 = X B
+  mm16(Mb + 16 * LD, LD, Xs, L16, nullptr, 0, 1.f, P2, L16, tid);      // P2 = C X
+  __syncthreads();
+  mm16(Mb + 16 * LD, LD, P1, L16, Mb + 16 * LD + 16, LD, -1.f, Ss, L16, tid);  // S = D - C P1
+  __syncthreads();
+  if (warp == 0) inv16_warp(Ss, L16, Ys, L16, lane, bad);
+  __syncthreads();
+  mm16(P1, L16, Ys, L16, nullptr, 0, -1.f, Ts + 16, LD, tid);            // T12 = -P1 Y
+  mm16(Ys, L16, P2, L16, nullptr, 0, -1.f, Ts + 16 * LD, LD, tid);       // T21 = -Y P2
+  Ts[(16 + (tid >> 4)) * LD + 16 + (tid & 15)] = Ys[(tid >> 4) * L16 + (tid & 15)];  // T22 = Y
+  __syncthreads();
+  mm16(P1, L16, Ts + 16 * LD, LD, Xs, L16, -1.f, Ts, LD, tid);          // T11 = X - P1 T21
+  __syncthreads();
+  if (jn < NB) {
+    const int r = tid >> 3, cq = tid & 7;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int c = cq + 8 * q;
+      if (r >= jn || c >= jn) Ts[r * LD + c] = make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+  }
+}
+
+// what the pivot-block server of a Gauss-Jordan step needs: the current
+// block inverse (Tin), where the next one goes (Tout), the next pivot block
+// J' = [j1, j1 + jn1) and, at the last step of a slice, the next slice's
+// stencil, permittivity and right-lead block (its first pivot block is then
+// A_{n+1}(J', J') - g_n(J', J') [- G0_R(J', J')])
+struct GjNext {
+  const float2* Tin;
+  float2* Tout;
+  int j1, jn1;
+  int next_slice;        // 1: J' is the next slice's first block
+  int same_block;        // 1: J' is the current block (one block per slice)
+  const double2* eps_next;
+  const double2* g0r;    // non-null: subtract G0_R(J', J') (the next slice is the last)
+  int64_t ldg;           // leading dimension of g0r (N)
+  const int* st_col;
+  const double2* st_val;
+  double2 k2;
+};
+
+// The pivot-block server (one CTA of the step's grid): the next pivot block
+// after this step, W_{j+1}(J', J') = W(J', J') - W(J', J) T W(J, J') (J' and J
+// disjoint), or T itself when J' = J, assembled with the next slice's matrix
+// at a slice boundary, then its inverse into ns.Tout -- computed while the
+// tile CTAs apply this step, so that the next step starts with its T ready.
+__device__ void t_server(const float* __restrict__ Wsrc, int64_t lda, int j0, int jn, const GjNext& ns,
+                         uint8_t* gb, int* bad) {
+  constexpr int LD = NB + 1;
+  const int tid = threadIdx.x, r = tid >> 3, cq = tid & 7;
+  float2* Tj = reinterpret_cast<float2*>(gb);
+  float2* B1 = Tj + NB * LD;  // W(J, J')
+  float2* B2 = B1 + NB * LD;  // W(J', J)
+  float2* B3 = B2 + NB * LD;  // W(J', J')
+  float2* U1 = B3 + NB * LD;
+  float2* Mn = U1 + NB * LD;
+  float2* To = Mn + NB * LD;
+  float2* tmp = To + NB * LD;
+  const int j1 = ns.j1, jn1 = ns.jn1;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int c = cq + 8 * q;
+    Tj[r * LD + c] = ns.Tin[r * NB + c];
+    const float2 z = make_float2(0.f, 0.f);
+    B1[r * LD + c] = (r < jn && c < jn1) ? *reinterpret_cast<const float2*>(Wsrc + (int64_t)(j0 + r) * lda + 2 * (j1 + c)) : z;
+    B2[r * LD + c] = (r < jn1 && c < jn) ? *reinterpret_cast<const float2*>(Wsrc + (int64_t)(j1 + r) * lda + 2 * (j0 + c)) : z;
+    B3[r * LD + c] = (r < jn1 && c < jn1) ? *reinterpret_cast<const float2*>(Wsrc + (int64_t)(j1 + r) * lda + 2 * (j1 + c)) : z;
+  }
+  __syncthreads();
+  if (!ns.same_block) {
+    mm32(Tj, B1, nullptr, 1.f, U1, tid);  // U1 = T W(J, J')
+    __syncthreads();
+    mm32(B2, U1, B3, -1.f, Mn, tid);      // W(J', J') - W(J', J) U1
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; q++) Mn[r * LD + cq + 8 * q] = Tj[r * LD + cq + 8 * q];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int c = cq + 8 * q;
+    float2 v = Mn[r * LD + c];
+    if (r < jn1 && c < jn1) {
+      if (ns.next_slice) {  // A_{n+1}(J', J') - g_n(J', J') [- G0_R(J', J')]
+        double2 a = cmk(-(double)v.x, -(double)v.y);
+        const int gi = j1 + r, gc = j1 + c;
+#pragma unroll
+        for (int qq = 0; qq < kMaxStencil; qq++)
+          if (ns.st_col[gi * kMaxStencil + qq] == gc) a = cadd(a, ns.st_val[gi * kMaxStencil + qq]);
+        if (gi == gc) a = csub(a, cmul(ns.k2, ns.eps_next[gi]));
+        if (ns.g0r) a = csub(a, ns.g0r[gi * ns.ldg + gc]);
+        v = make_float2((float)a.x, (float)a.y);
+      }
+    } else {
+      v = make_float2(r == c ? 1.f : 0.f, 0.f);
+    }
+    Mn[r * LD + c] = v;
+  }
+  __syncthreads();
+  inv32_block(Mn, To, tmp, jn1, tid, bad);
+#pragma unroll
+  for (int q = 0; q < 4; q++) ns.Tout[r * NB + cq + 8 * q] = To[r * LD + cq + 8 * q];
+}
+
 __global__ void __launch_bounds__(256, 1)
     k_mx_gj_step(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapW,
                  const float* __restrict__ Wsrc, float* __restrict__ Wdst, int64_t lda, int N, int j0, int jn,
-                 int* status, long long timeout) {
+                 const GjNext ns, int* status, long long timeout) {
   using namespace gjs;
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t bar_ld;
@@ -485,6 +639,16 @@ __global__ void __launch_bounds__(256, 1)
   const uint32_t sb = (tc32::su32(smem_raw) + 1023u) & ~1023u;
   uint8_t* gb = smem_raw + (sb - tc32::su32(smem_raw));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (blockIdx.x == gridDim.x - 1) {  // the last grid column: the pivot-block server (row 0) only
+    if (blockIdx.y != 0) return;
+    if (tid == 0) bad = 0;
+    pdl_wait();
+    __syncthreads();
+    if (ns.Tout) t_server(Wsrc, lda, j0, jn, ns, gb, &bad);
+    __syncthreads();
+    if (bad && tid == 0) atomicOr(status, kStatusSingular);
+    return;
+  }
   const int m0 = blockIdx.y * 128, n0 = blockIdx.x * BN;
   if (tid == 0) {
     tc32::mbar_init(tc32::su32(&bar_ld), 1);
@@ -513,14 +677,13 @@ __global__ void __launch_bounds__(256, 1)
     for (int kc = 0; kc < 2; kc++) tc32::tma_load_3d(sb + OFF_AH + kc * CH, &mapA, 2 * j0 + 32 * kc, m0, 0, bl);
     for (int kc = 0; kc < 4; kc++) tc32::tma_load_3d(sb + OFF_WP + kc * CH, &mapW, n0 + 32 * kc, m0, 0, bl);
   }
-  // (2) the pivot block (thread: row tid/8, columns tid%8 + 8q) and W(J, tile columns) into registers
-  const int r = tid >> 3, cq = tid & 7;
-  float2 a[4];
+  // (2) this step's pivot-block inverse (from the server of the step before)
+  //     and W(J, tile columns) into registers
+  float2* Ts = reinterpret_cast<float2*>(gb + OFF_T);
+  {
+    const int r = tid >> 3, cq = tid & 7;
 #pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const int c = cq + 8 * q;
-    a[q] = (r < jn && c < jn) ? *reinterpret_cast<const float2*>(Wsrc + (int64_t)(j0 + r) * lda + 2 * (j0 + c))
-                              : make_float2(0.f, 0.f);
+    for (int q = 0; q < 4; q++) Ts[r * (NB + 1) + cq + 8 * q] = ns.Tin[r * NB + cq + 8 * q];
   }
   float4 wj[4];
 #pragma unroll
@@ -530,49 +693,6 @@ __global__ void __launch_bounds__(256, 1)
                                   : make_float4(0.f, 0.f, 0.f, 0.f);
   }
   MX_STAMP(2);
-  // (3) T = W(J, J)^-1 by 2 x 2 blocks of 16 (A, B; C, D): X = A^-1,
-  //     S = D - C X B, Y = S^-1, T = [[X - X B T21, -X B Y], [-Y C X, Y]];
-  //     the inverses by warp 0 (shuffles only), the products by all threads.
-  //     The block is identity-padded beyond jn and T zeroed there.  The
-  //     temporaries live in the A_lo operand area, written only later.
-  float2* Ts = reinterpret_cast<float2*>(gb + OFF_T);
-  {
-    constexpr int LD = NB + 1, L16 = 17;
-    float2* Mb = reinterpret_cast<float2*>(gb + OFF_AL);
-    float2* Xs = Mb + NB * LD;
-    float2* P1 = Xs + 16 * L16;
-    float2* P2 = P1 + 16 * L16;
-    float2* Ss = P2 + 16 * L16;
-    float2* Ys = Ss + 16 * L16;
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const int c = cq + 8 * q;
-      Mb[r * LD + c] = (r < jn && c < jn) ? a[q] : make_float2(r == c ? 1.f : 0.f, 0.f);
-    }
-    __syncthreads();
-    if (warp == 0) inv16_warp(Mb, LD, Xs, L16, lane, &bad);
-    __syncthreads();
-    mm16(Xs, L16, Mb + 16, LD, nullptr, 0, 1.f, P1, L16, tid);           // P1 = X B
-    mm16(Mb + 16 * LD, LD, Xs, L16, nullptr, 0, 1.f, P2, L16, tid);      // P2 = C X
-    __syncthreads();
-    mm16(Mb + 16 * LD, LD, P1, L16, Mb + 16 * LD + 16, LD, -1.f, Ss, L16, tid);  // S = D - C P1
-    __syncthreads();
-    if (warp == 0) inv16_warp(Ss, L16, Ys, L16, lane, &bad);
-    __syncthreads();
-    mm16(P1, L16, Ys, L16, nullptr, 0, -1.f, Ts + 16, LD, tid);            // T12 = -P1 Y
-    mm16(Ys, L16, P2, L16, nullptr, 0, -1.f, Ts + 16 * LD, LD, tid);       // T21 = -Y P2
-    Ts[(16 + (tid >> 4)) * LD + 16 + (tid & 15)] = Ys[(tid >> 4) * L16 + (tid & 15)];  // T22 = Y
-    __syncthreads();
-    mm16(P1, L16, Ts + 16 * LD, LD, Xs, L16, -1.f, Ts, LD, tid);          // T11 = X - P1 T21
-    __syncthreads();  // the temporaries are overwritten by the operand split below
-    if (jn < NB) {
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const int c = cq + 8 * q;
-        if (r >= jn || c >= jn) Ts[r * LD + c] = make_float2(0.f, 0.f);
-      }
-    }
-  }
   MX_STAMP(3);
   // W'(J, tile columns): the pivot columns replaced by the identity's
   float2* Wj = reinterpret_cast<float2*>(gb + OFF_WJC);
@@ -697,11 +817,36 @@ __global__ void __launch_bounds__(256, 1)
     }
   }
   MX_STAMP(9);
-  if (bad && tid == 0 && blockIdx.x == 0 && blockIdx.y == 0) atomicOr(status, kStatusSingular);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
+}
+
+// the first pivot-block inverse of the first slice (later ones come from the
+// step kernels' server): T = W(J0, J0)^-1, one CTA
+__global__ void __launch_bounds__(256) k_mx_t0(const float* __restrict__ W, int64_t lda, int jn, float2* Tout,
+                                               int* status) {
+  pdl_open();
+  pdl_wait();
+  constexpr int LD = NB + 1;
+  __shared__ float2 Mb[NB * LD];
+  __shared__ float2 To[NB * LD];
+  __shared__ float2 tmp[5 * 16 * 17];
+  __shared__ int bad;
+  const int tid = threadIdx.x, r = tid >> 3, cq = tid & 7;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int c = cq + 8 * q;
+    Mb[r * LD + c] = (r < jn && c < jn) ? *reinterpret_cast<const float2*>(W + (int64_t)r * lda + 2 * c)
+                                        : make_float2(r == c ? 1.f : 0.f, 0.f);
+  }
+  if (tid == 0) bad = 0;
+  __syncthreads();
+  inv32_block(Mb, To, tmp, jn, tid, &bad);
+#pragma unroll
+  for (int q = 0; q < 4; q++) Tout[r * NB + cq + 8 * q] = To[r * LD + cq + 8 * q];
+  if (bad && tid == 0) atomicOr(status, kStatusSingular);
 }
 
 inline int64_t lda_of(int64_t N) { return (2 * N + 31) / 32 * 32; }
@@ -758,9 +903,10 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  // solve GEMM tile width: the narrowest of 64 / 128 / 256 real columns that
-  // covers the request in one or two tiles keeps the factor's re-reads low
-  const int sbn = (2 * P <= 64) ? 64 : (2 * P <= 128) ? 128 : 256;
+  // solve GEMM tile width: 64 real columns for narrow requests, else 128 (a
+  // three-deep TMA pipeline; 256-wide tiles leave room for two stages only
+  // and stall on the loads)
+  const int sbn = (2 * P <= 64) ? 64 : 128;
   if ((st = gemm_attr<64>()) || (st = gemm_attr<128>()) || (st = gemm_attr<256>())) return st;
   if (cudaFuncSetAttribute(k_mx_gj_step, cudaFuncAttributeMaxDynamicSharedMemorySize, gjs::SMEM) != cudaSuccess) {
     set_error("cannot configure the Gauss-Jordan step kernel's shared memory");
@@ -768,26 +914,40 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
   }
   void *pW, *pSh, *pSl, *pX, *pY, *pPart, *pBt, *pVec, *pNorm, *pStat;
   const int ntile_m = (int)((N + tc32::BM - 1) / tc32::BM);
-  const int ntile_s = (int)((2 * P + sbn - 1) / sbn);
+  // the solve's columns are independent: wide requests run as two column
+  // groups on two streams (each sweep is latency-bound, so the two overlap)
   const int kchunks = (int)(lda / tc32::BK);
-  const int ksplit = choose_ksplit((int64_t)ntile_m * ntile_s, kchunks, sms);
-  if ((st = alloc(kMxW, 2 * sizeof(float) * N * lda, &pW)) ||
+  const int ngrp = P >= 64 ? 2 : 1;
+  int64_t gP[2] = {P, 0}, gOff[2] = {0, 0};
+  int gTiles[2] = {0, 0}, gSplit[2] = {1, 1};
+  if (ngrp == 2) {
+    gP[0] = (P + 1) / 2;
+    gP[1] = P - gP[0];
+    gOff[1] = gP[0];
+  }
+  int64_t part_elems = 0;
+  for (int g = 0; g < ngrp; g++) {
+    gTiles[g] = (int)((2 * gP[g] + sbn - 1) / sbn);
+    gSplit[g] = choose_ksplit((int64_t)ntile_m * gTiles[g], kchunks, sms / ngrp);
+    part_elems += N * gP[g] * gSplit[g];
+  }
+  void* pT = nullptr;
+  if ((st = alloc(kMxW, 2 * sizeof(float) * N * lda, &pW)) || (st = alloc(kMxT, sizeof(float2) * 2 * NB * NB, &pT)) ||
       (st = alloc(kMxStoreHi, sizeof(float) * N * lda * L, &pSh)) ||
       (st = alloc(kMxStoreLo, sizeof(float) * N * lda * L, &pSl)) ||
       (st = alloc(kMxX, sizeof(double2) * NP * L, &pX)) || (st = alloc(kMxY, sizeof(float2) * NP * L, &pY)) ||
-      (st = alloc(kMxPart, sizeof(float2) * NP * ksplit, &pPart)) ||
+      (st = alloc(kMxPart, sizeof(float2) * part_elems, &pPart)) ||
       (st = alloc(kMxBt, 2 * sizeof(float) * 2 * P * lda, &pBt)) ||
       (st = alloc(kMxVec, sizeof(double2) * NP * 6, &pVec)) || (st = alloc(kMxNorm, sizeof(double) * 8, &pNorm)) ||
       (st = alloc(kMxStatus, sizeof(int), &pStat)))
     return st;
   float* Wb[2] = {static_cast<float*>(pW), static_cast<float*>(pW) + N * lda};
+  float2* Tbuf = static_cast<float2*>(pT);  // two pivot-block inverses (step parity)
   float* st_hi = static_cast<float*>(pSh);
   float* st_lo = static_cast<float*>(pSl);
   double2* x = static_cast<double2*>(pX);
   float2* y = static_cast<float2*>(pY);
-  float2* part = static_cast<float2*>(pPart);
   float* bt_hi = static_cast<float*>(pBt);
-  float* bt_lo = bt_hi + 2 * P * lda;
   double2* Bl = static_cast<double2*>(pVec);
   double2* Br = Bl + NP;
   double2* b0 = Br + NP;
@@ -800,21 +960,37 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
   // tensor maps: the two W buffers (swizzled 32-column boxes for the update's
   // left operand, unswizzled ones for the W' tile), the factor store (N rows x
   // lda, L slices) and the solve's right operand (2P rows x lda)
-  CUtensorMap mA[2], mWp[2], mSh, mSl, mBh, mBl;
+  CUtensorMap mA[2], mWp[2], mSh, mSl, mBh[2], mBl[2];
+  float* gBh[2] = {nullptr, nullptr};
+  float* gBl[2] = {nullptr, nullptr};
+  float2* gPart[2] = {nullptr, nullptr};
+  {
+    float* bp = bt_hi;
+    float2* pp = static_cast<float2*>(pPart);
+    for (int g = 0; g < ngrp; g++) {
+      gBh[g] = bp;
+      gBl[g] = bp + 2 * gP[g] * lda;
+      bp += 4 * gP[g] * lda;
+      gPart[g] = pp;
+      pp += N * gP[g] * gSplit[g];
+    }
+  }
+  bool maps_ok = true;
+  for (int g = 0; g < ngrp; g++)
+    maps_ok = maps_ok && tc32::make_map(&mBh[g], gBh[g], lda, 2 * gP[g], 1, lda, 0, sbn) &&
+              tc32::make_map(&mBl[g], gBl[g], lda, 2 * gP[g], 1, lda, 0, sbn);
   if (!(tc32::make_map(&mA[0], Wb[0], lda, N, 1, lda, 0, tc32::BM) &&
         tc32::make_map(&mA[1], Wb[1], lda, N, 1, lda, 0, tc32::BM) &&
         tc32::make_map(&mWp[0], Wb[0], lda, N, 1, lda, 0, tc32::BM, CU_TENSOR_MAP_SWIZZLE_NONE) &&
         tc32::make_map(&mWp[1], Wb[1], lda, N, 1, lda, 0, tc32::BM, CU_TENSOR_MAP_SWIZZLE_NONE) &&
         tc32::make_map(&mSh, st_hi, lda, N, L, lda, N * lda, tc32::BM) &&
-        tc32::make_map(&mSl, st_lo, lda, N, L, lda, N * lda, tc32::BM) &&
-        tc32::make_map(&mBh, bt_hi, lda, 2 * P, 1, lda, 0, sbn) &&
-        tc32::make_map(&mBl, bt_lo, lda, 2 * P, 1, lda, 0, sbn))) {
+        tc32::make_map(&mSl, st_lo, lda, N, L, lda, N * lda, tc32::BM) && maps_ok)) {
     set_error("tensor-map encoding for the tcgen05 GEMM failed");
     return RGF_ERR_CUDA;
   }
   RGF_CUDA_TRY_MX(cudaMemsetAsync(mstat, 0, sizeof(int), s));
   RGF_CUDA_TRY_MX(cudaMemsetAsync(Wb[0], 0, 2 * sizeof(float) * N * lda, s));
-  RGF_CUDA_TRY_MX(cudaMemsetAsync(bt_hi, 0, 2 * sizeof(float) * 2 * P * lda, s));
+  RGF_CUDA_TRY_MX(cudaMemsetAsync(bt_hi, 0, 2 * sizeof(float) * 2 * P * lda, s));  // zero K padding of every group
   RGF_CUDA_TRY_MX(cudaMemsetAsync(x, 0, sizeof(double2) * NP * L, s));
   cudaEvent_t ev[3];
   for (int q = 0; q < 3; q++) RGF_CUDA_TRY_MX(cudaEventCreate(&ev[q]));
@@ -829,8 +1005,11 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
   // (1) low-precision factorization
   RGF_CUDA_TRY_MX(cudaEventRecord(ev[0], s));
   const dim3 ga((unsigned)((ldw + 255) / 256), (unsigned)std::min<int64_t>(N, 8192));
-  const dim3 ggj((unsigned)((lda + gjs::BN - 1) / gjs::BN), (unsigned)ntile_m);
-  int cur = 0;  // W buffer holding the current matrix
+  // one grid column more than the tiles: its first CTA serves the next pivot block
+  const dim3 ggj((unsigned)((lda + gjs::BN - 1) / gjs::BN + 1), (unsigned)ntile_m);
+  const int64_t nsteps = (N + NB - 1) / NB;
+  int cur = 0;      // W buffer holding the current matrix
+  int64_t gstep = 0;  // steps issued so far (parity selects the pivot-block inverse buffer)
   for (int64_t k = 0; k < L; k++) {
     const double2* Ga = (k == 0) ? mp.G0[0] : nullptr;
     const double2* Gb = (k == L - 1) ? mp.G0[1] : nullptr;
@@ -839,11 +1018,37 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
     launch_pdl(k_mx_assemble, ga, dim3(256), 0, s, reinterpret_cast<float2*>(Wb[cur]), ldw, N, sh, sl, (int)(k > 0),
                1, mp.st_col, mp.st_val, mp.k2, mp.eps + k * N, Ga, Gb);
     nl++;
+    if (k == 0) {
+      launch_pdl(k_mx_t0, dim3(1), dim3(256), 0, s, (const float*)Wb[cur], lda, (int)std::min<int64_t>(NB, N), Tbuf,
+                 mstat);
+      nl++;
+    }
     for (int64_t j0 = 0; j0 < N; j0 += NB) {
       const int jn = (int)std::min<int64_t>(NB, N - j0);
+      GjNext ns{};
+      ns.Tin = Tbuf + (gstep & 1) * NB * NB;
+      ns.Tout = Tbuf + ((gstep + 1) & 1) * NB * NB;
+      ns.st_col = mp.st_col;
+      ns.st_val = mp.st_val;
+      ns.k2 = mp.k2;
+      ns.ldg = N;
+      if (j0 + NB < N) {
+        ns.j1 = (int)(j0 + NB);
+        ns.jn1 = (int)std::min<int64_t>(NB, N - j0 - NB);
+      } else if (k + 1 < L) {  // the next slice's first block
+        ns.j1 = 0;
+        ns.jn1 = (int)std::min<int64_t>(NB, N);
+        ns.next_slice = 1;
+        ns.same_block = nsteps == 1;
+        ns.eps_next = mp.eps + (k + 1) * N;
+        ns.g0r = (k + 1 == L - 1) ? mp.G0[1] : nullptr;
+      } else {
+        ns.Tout = nullptr;  // the last step of the last slice: nothing follows
+      }
       launch_pdl(k_mx_gj_step, ggj, dim3(256), gjs::SMEM, s, mA[cur], mWp[cur], (const float*)Wb[cur],
-                 Wb[cur ^ 1], lda, (int)N, (int)j0, jn, mstat, kGemmTimeout);
+                 Wb[cur ^ 1], lda, (int)N, (int)j0, jn, ns, mstat, kGemmTimeout);
       cur ^= 1;
+      gstep++;
       nl++;
     }
   }
@@ -863,27 +1068,49 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
   nl += 3;
 
   // (3) refinement
-  tc32::GemmArgs gs{};
-  gs.M = (int)N;
-  gs.Nr = (int)(2 * P);
-  gs.k_chunks = kchunks / ksplit;
-  gs.mode = tc32::kPartial;
-  gs.out = reinterpret_cast<float*>(part);
-  gs.ldo = 2 * P;
-  gs.split_stride = 2 * NP;
-  gs.err = mstat;
-  gs.timeout = kGemmTimeout;
-  const dim3 gsg((unsigned)ntile_s, (unsigned)ntile_m, (unsigned)ksplit);
-  const dim3 gp((unsigned)((P + 31) / 32), (unsigned)((N + 31) / 32));
+  tc32::GemmArgs gs[2];
+  dim3 gsg[2], gp[2];
+  cudaStream_t gst[2] = {s, nullptr};
+  cudaEvent_t fork = nullptr, join = nullptr;
+  struct StreamGuard {
+    cudaStream_t* st;
+    cudaEvent_t* f;
+    cudaEvent_t* j;
+    ~StreamGuard() {
+      if (*st) cudaStreamDestroy(*st);
+      if (*f) cudaEventDestroy(*f);
+      if (*j) cudaEventDestroy(*j);
+    }
+  } sg{&gst[1], &fork, &join};
+  if (ngrp == 2) {
+    RGF_CUDA_TRY_MX(cudaStreamCreateWithFlags(&gst[1], cudaStreamNonBlocking));
+    RGF_CUDA_TRY_MX(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    RGF_CUDA_TRY_MX(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+  }
+  for (int g = 0; g < ngrp; g++) {
+    gs[g] = tc32::GemmArgs{};
+    gs[g].M = (int)N;
+    gs[g].Nr = (int)(2 * gP[g]);
+    gs[g].k_chunks = kchunks / gSplit[g];
+    gs[g].mode = tc32::kPartial;
+    gs[g].out = reinterpret_cast<float*>(gPart[g]);
+    gs[g].ldo = 2 * gP[g];
+    gs[g].split_stride = 2 * N * gP[g];
+    gs[g].err = mstat;
+    gs[g].timeout = kGemmTimeout;
+    gsg[g] = dim3((unsigned)gTiles[g], (unsigned)ntile_m, (unsigned)gSplit[g]);
+    gp[g] = dim3((unsigned)((gP[g] + 31) / 32), (unsigned)((N + 31) / 32));
+  }
   const dim3 tp(32, 8);
-  auto gemm = [&](int64_t k) {
-    gs.a_z = (int)k;
+  auto gemm = [&](int g, int64_t k) {
+    gs[g].a_z = (int)k;
+    cudaStream_t q = gst[g];
     if (sbn == 64)
-      launch_pdl(tc32::k_tc32_gemm<64>, gsg, dim3(tc32::kThreads), tc32::Cfg<64>::SMEM, s, mSh, mSl, mBh, mBl, gs);
-    else if (sbn == 128)
-      launch_pdl(tc32::k_tc32_gemm<128>, gsg, dim3(tc32::kThreads), tc32::Cfg<128>::SMEM, s, mSh, mSl, mBh, mBl, gs);
+      launch_pdl(tc32::k_tc32_gemm<64>, gsg[g], dim3(tc32::kThreads), tc32::Cfg<64>::SMEM, q, mSh, mSl, mBh[g],
+                 mBl[g], gs[g]);
     else
-      launch_pdl(tc32::k_tc32_gemm<256>, gsg, dim3(tc32::kThreads), tc32::Cfg<256>::SMEM, s, mSh, mSl, mBh, mBl, gs);
+      launch_pdl(tc32::k_tc32_gemm<128>, gsg[g], dim3(tc32::kThreads), tc32::Cfg<128>::SMEM, q, mSh, mSl, mBh[g],
+                 mBl[g], gs[g]);
   };
   double prev = 1.0, change = 1.0;
   bool conv = false;
@@ -901,19 +1128,32 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
                (const double2*)b0, (const double2*)bL, (const double2*)(have_x ? e0 : nullptr),
                (const double2*)(have_x ? e1 : nullptr));
     nl++;
-    for (int64_t k = 0; k < L; k++) {
-      launch_pdl(k_mx_fwd_prep, gp, tp, 0, s, k, N, P, y, (const float2*)part, ksplit, bt_hi, bt_lo, lda);
-      gemm(k);
-      nl += 2;
+    if (ngrp == 2) {
+      RGF_CUDA_TRY_MX(cudaEventRecord(fork, s));
+      RGF_CUDA_TRY_MX(cudaStreamWaitEvent(gst[1], fork, 0));
     }
-    for (int64_t k = L - 1; k >= 0; k--) {
-      launch_pdl(k_mx_bwd_prep, gp, tp, 0, s, k, L, N, P, x, (const float2*)y, (const float2*)part, ksplit, bt_hi,
-                 bt_lo, lda, norms);
-      nl++;
-      if (k > 0) {
-        gemm(k - 1);
-        nl++;
+    // forward then backward substitution; the column groups' launches
+    // interleaved slice by slice so that both streams are fed
+    for (int64_t k = 0; k < L; k++)
+      for (int g = 0; g < ngrp; g++) {
+        launch_pdl(k_mx_fwd_prep, gp[g], tp, 0, gst[g], k, N, gP[g], P, gOff[g], y, (const float2*)gPart[g],
+                   gSplit[g], gBh[g], gBl[g], lda);
+        gemm(g, k);
+        nl += 2;
       }
+    for (int64_t k = L - 1; k >= 0; k--)
+      for (int g = 0; g < ngrp; g++) {
+        launch_pdl(k_mx_bwd_prep, gp[g], tp, 0, gst[g], k, L, N, gP[g], P, gOff[g], x, (const float2*)y,
+                   (const float2*)gPart[g], gSplit[g], gBh[g], gBl[g], lda, norms);
+        nl++;
+        if (k > 0) {
+          gemm(g, k - 1);
+          nl++;
+        }
+      }
+    if (ngrp == 2) {
+      RGF_CUDA_TRY_MX(cudaEventRecord(join, gst[1]));
+      RGF_CUDA_TRY_MX(cudaStreamWaitEvent(s, join, 0));
     }
     RGF_CUDA_TRY_MX(cudaGetLastError());
     double hn[8];

@@ -39,7 +39,7 @@ struct MixedStats {
 
 // device workspace slots the precision form asks its caller for
 enum MixedSlot : int {
-  kMxW, kMxStoreHi, kMxStoreLo, kMxX, kMxY, kMxPart, kMxBt, kMxVec, kMxNorm, kMxStatus,
+  kMxW, kMxT, kMxStoreHi, kMxStoreLo, kMxX, kMxY, kMxPart, kMxBt, kMxVec, kMxNorm, kMxStatus,
   kMxSlots
 };
 using MixedAlloc = std::function<rgf_status(int slot, size_t bytes, void** p)>;
