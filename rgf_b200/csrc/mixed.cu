@@ -81,6 +81,10 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;"
 
 // launch with programmatic stream serialization (every kernel launched this
 // way waits for its predecessor with pdl_wait before it reads or writes)
+// off while two streams run the two sides at once: a stream's early-launched,
+// waiting CTAs would hold SMs that the other stream's kernels need
+thread_local bool t_use_pdl = true;
+
 template <typename... KArgs, typename... Args>
 cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
                        Args&&... args) {
@@ -93,7 +97,7 @@ cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t sme
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = t_use_pdl ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
@@ -103,11 +107,12 @@ cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t sme
 
 // W holds g_{k-1} (store != 0: written to the factor store as hi/lo) and is
 // replaced by the next slice matrix (assemble != 0):
-//   W = A_k - g_{k-1} - Ga - Gb,  A_k = stencil - k0dx^2 eps_k on the diagonal.
+//   W = A_k - g_{k-1} - Ga - Gb - Wx,  A_k = stencil - k0dx^2 eps_k on the diagonal
+// (Wx: the block of the other side at the junction slice of the two-sided form).
 // Columns [N, ldw) are the zero padding of the store rows.
 __global__ void k_mx_assemble(float2* W, int64_t ldw, int64_t N, float* st_hi, float* st_lo, int store,
                               int assemble, const int* st_col, const double2* st_val, double2 k2,
-                              const double2* eps, const double2* Ga, const double2* Gb) {
+                              const double2* eps, const double2* Ga, const double2* Gb, const float2* Wx) {
   pdl_open();
   pdl_wait();
   const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -127,6 +132,7 @@ __global__ void k_mx_assemble(float2* W, int64_t ldw, int64_t N, float* st_hi, f
     double2 v = store ? cmk(-(double)w.x, -(double)w.y) : cmk(0.0, 0.0);
     if (Ga) v = csub(v, Ga[i * N + j]);
     if (Gb) v = csub(v, Gb[i * N + j]);
+    if (Wx) v = cmk(v.x - (double)Wx[o].x, v.y - (double)Wx[o].y);  // the other side's block (junction slice)
 #pragma unroll
     for (int q = 0; q < kMaxStencil; q++)
       if (st_col[i * kMaxStencil + q] == j) v = cadd(v, st_val[i * kMaxStencil + q]);
@@ -205,13 +211,19 @@ __global__ void __launch_bounds__(256) k_mx_residual(int64_t L, int64_t N, int64
   }
 }
 
-// forward pass, slice k: y_{k-1} = (GEMM partials) -> ystore[k-1] (over
-// r_{k-1}); v_k = r_k + y_{k-1} -> Bt.
-__global__ void __launch_bounds__(256) k_mx_fwd_prep(int64_t k, int64_t N, int64_t P, int64_t ldp, int64_t poff,
-                                                     float2* ystore, const float2* part, int ksplit, float* bt_hi,
-                                                     float* bt_lo, int64_t lda) {
+// forward pass, slice k: y_kprev = (GEMM partials) -> ystore[kprev] (over its
+// r; kprev = k -+ 1 by the sweep's direction, < 0 at the sweep's first slice);
+// v_k = r_k + y_kprev (+ y_kprev2 from part2 at the junction slice) -> Bt.
+__global__ void __launch_bounds__(256) k_mx_fwd_prep(int64_t k, int64_t kprev, int64_t N, int64_t P, int64_t ldp,
+                                                     int64_t poff, float2* ystore, const float2* part, int ksplit,
+                                                     const float2* part2, int64_t kprev2, int ksplit2, float* bt_hi,
+                                                     float* bt_lo, int64_t lda, const int* kdev) {
   pdl_open();
   pdl_wait();
+  if (kdev) {  // slice index kept on the device (graph-captured sweeps)
+    k += *kdev;
+    kprev += *kdev;
+  }
   __shared__ float2 tile[32][33];
   const int64_t p0 = blockIdx.x * 32, i0 = blockIdx.y * 32, NP = N * ldp;
   const int64_t p = p0 + threadIdx.x;
@@ -223,11 +235,17 @@ __global__ void __launch_bounds__(256) k_mx_fwd_prep(int64_t k, int64_t N, int64
     if (i < N && p < P) {
       const int64_t ip = i * ldp + poff + p;
       v = ystore[k * NP + ip];  // r_k
-      if (k > 0) {
+      if (kprev >= 0) {  // y of the neighbour slice swept before (over its r)
         const float2 yp = sum_parts(part, ksplit, N * P, i * P + p);
-        ystore[(k - 1) * NP + ip] = yp;
+        ystore[kprev * NP + ip] = yp;
         v.x += yp.x;
         v.y += yp.y;
+      }
+      if (part2) {  // junction slice: the other side's neighbour too
+        const float2 yq = sum_parts(part2, ksplit2, N * P, i * P + p);
+        ystore[kprev2 * NP + ip] = yq;
+        v.x += yq.x;
+        v.y += yq.y;
       }
     }
     tile[threadIdx.x][q] = v;
@@ -236,15 +254,21 @@ __global__ void __launch_bounds__(256) k_mx_fwd_prep(int64_t k, int64_t N, int64
   store_bt(tile, p0, i0, N, P, bt_hi, bt_lo, lda);
 }
 
-// backward pass, slice k: d_k = y_k + (GEMM partials) (k = L-1: the partials
-// are y_{L-1}); x_k += d_k in FP64; norms of d and x (whole; slice 0; slice
-// L-1); for k > 0 d_k -> Bt.
+// backward pass, slice k: d_k = (GEMM partials) + y_k (add_y; without it the
+// partials are d_k itself: the sweep's first slice); x_k += d_k in FP64; norms
+// of d and x (whole; slice 0; slice L-1); d_k -> Bt (write_bt) and -> Bt2 (the
+// junction slice feeds both sides).  add_y, write_bt < 0: the one-sided rule.
 __global__ void __launch_bounds__(256) k_mx_bwd_prep(int64_t k, int64_t L, int64_t N, int64_t P, int64_t ldp,
                                                      int64_t poff, double2* x,
                                                      const float2* ystore, const float2* part, int ksplit,
-                                                     float* bt_hi, float* bt_lo, int64_t lda, double* norms) {
+                                                     float* bt_hi, float* bt_lo, int64_t lda, double* norms,
+                                                     const int* kdev, int add_y, int write_bt, float* bt2_hi,
+                                                     float* bt2_lo) {
   pdl_open();
   pdl_wait();
+  if (kdev) k += *kdev;  // slice index kept on the device (graph-captured sweeps)
+  if (add_y < 0) add_y = k < L - 1;   // one-sided sweep: y_k enters except at the first slice
+  if (write_bt < 0) write_bt = k > 0;  // ... and the next GEMM needs d_k except after slice 0
   __shared__ float2 tile[32][33];
   __shared__ double red[2][8];
   const int64_t p0 = blockIdx.x * 32, i0 = blockIdx.y * 32, NP = N * ldp;
@@ -258,7 +282,7 @@ __global__ void __launch_bounds__(256) k_mx_bwd_prep(int64_t k, int64_t L, int64
     if (i < N && p < P) {
       const int64_t ip = i * ldp + poff + p;
       d = sum_parts(part, ksplit, N * P, i * P + p);
-      if (k < L - 1) {
+      if (add_y) {
         const float2 y = ystore[k * NP + ip];
         d.x += y.x;
         d.y += y.y;
@@ -297,7 +321,8 @@ __global__ void __launch_bounds__(256) k_mx_bwd_prep(int64_t k, int64_t L, int64
       atomicAdd(norms + 5, b);
     }
   }
-  if (k > 0) store_bt(tile, p0, i0, N, P, bt_hi, bt_lo, lda);
+  if (write_bt) store_bt(tile, p0, i0, N, P, bt_hi, bt_lo, lda);
+  if (bt2_hi) store_bt(tile, p0, i0, N, P, bt2_hi, bt2_lo, lda);
 }
 
 // B columns in S order: left inputs into Bl, right inputs into Br (N x P row-major)
@@ -912,37 +937,30 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
     set_error("cannot configure the Gauss-Jordan step kernel's shared memory");
     return RGF_ERR_CUDA;
   }
-  void *pW, *pSh, *pSl, *pX, *pY, *pPart, *pBt, *pVec, *pNorm, *pStat;
+  void *pW, *pT, *pSh, *pSl, *pX, *pY, *pPart, *pBt, *pVec, *pNorm, *pStat;
   const int ntile_m = (int)((N + tc32::BM - 1) / tc32::BM);
-  // the solve's columns are independent: wide requests run as two column
-  // groups on two streams (each sweep is latency-bound, so the two overlap)
   const int kchunks = (int)(lda / tc32::BK);
-  const int ngrp = P >= 64 ? 2 : 1;
-  int64_t gP[2] = {P, 0}, gOff[2] = {0, 0};
-  int gTiles[2] = {0, 0}, gSplit[2] = {1, 1};
-  if (ngrp == 2) {
-    gP[0] = (P + 1) / 2;
-    gP[1] = P - gP[0];
-    gOff[1] = gP[0];
-  }
-  int64_t part_elems = 0;
-  for (int g = 0; g < ngrp; g++) {
-    gTiles[g] = (int)((2 * gP[g] + sbn - 1) / sbn);
-    gSplit[g] = choose_ksplit((int64_t)ntile_m * gTiles[g], kchunks, sms / ngrp);
-    part_elems += N * gP[g] * gSplit[g];
-  }
-  void* pT = nullptr;
-  if ((st = alloc(kMxW, 2 * sizeof(float) * N * lda, &pW)) || (st = alloc(kMxT, sizeof(float2) * 2 * NB * NB, &pT)) ||
+  // Two-sided form (L >= 8): the slices [0, c-1) are factored from the left
+  // lead and [c, L) from the right lead, concurrently on two streams; the
+  // junction slice c-1 is then inverted with both sides' blocks,
+  // (A_{c-1} - g_{c-2} - g_c)^-1, and every solve sweeps both halves at once
+  // and meets there.  Below 8 slices one chain from the left (the reference's
+  // order) does it all.
+  const bool two = L >= 8;
+  const int64_t cj = two ? (L + 1) / 2 : L;  // junction slice + 1 (two-sided)
+  const int nside = two ? 2 : 1;
+  int sTiles = (int)((2 * P + sbn - 1) / sbn);
+  int sSplit = choose_ksplit((int64_t)ntile_m * sTiles, kchunks, sms / nside);
+  if ((st = alloc(kMxW, 2 * nside * sizeof(float) * N * lda, &pW)) ||
+      (st = alloc(kMxT, sizeof(float2) * 2 * nside * NB * NB, &pT)) ||
       (st = alloc(kMxStoreHi, sizeof(float) * N * lda * L, &pSh)) ||
       (st = alloc(kMxStoreLo, sizeof(float) * N * lda * L, &pSl)) ||
       (st = alloc(kMxX, sizeof(double2) * NP * L, &pX)) || (st = alloc(kMxY, sizeof(float2) * NP * L, &pY)) ||
-      (st = alloc(kMxPart, sizeof(float2) * part_elems, &pPart)) ||
-      (st = alloc(kMxBt, 2 * sizeof(float) * 2 * P * lda, &pBt)) ||
+      (st = alloc(kMxPart, sizeof(float2) * NP * sSplit * nside, &pPart)) ||
+      (st = alloc(kMxBt, 2 * nside * sizeof(float) * 2 * P * lda, &pBt)) ||
       (st = alloc(kMxVec, sizeof(double2) * NP * 6, &pVec)) || (st = alloc(kMxNorm, sizeof(double) * 8, &pNorm)) ||
-      (st = alloc(kMxStatus, sizeof(int), &pStat)))
+      (st = alloc(kMxStatus, 4 * sizeof(int), &pStat)))
     return st;
-  float* Wb[2] = {static_cast<float*>(pW), static_cast<float*>(pW) + N * lda};
-  float2* Tbuf = static_cast<float2*>(pT);  // two pivot-block inverses (step parity)
   float* st_hi = static_cast<float*>(pSh);
   float* st_lo = static_cast<float*>(pSl);
   double2* x = static_cast<double2*>(pX);
@@ -957,40 +975,84 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
   double* norms = static_cast<double*>(pNorm);
   int* mstat = static_cast<int*>(pStat);
 
-  // tensor maps: the two W buffers (swizzled 32-column boxes for the update's
-  // left operand, unswizzled ones for the W' tile), the factor store (N rows x
-  // lda, L slices) and the solve's right operand (2P rows x lda)
-  CUtensorMap mA[2], mWp[2], mSh, mSl, mBh[2], mBl[2];
-  float* gBh[2] = {nullptr, nullptr};
-  float* gBl[2] = {nullptr, nullptr};
-  float2* gPart[2] = {nullptr, nullptr};
-  {
-    float* bp = bt_hi;
-    float2* pp = static_cast<float2*>(pPart);
-    for (int g = 0; g < ngrp; g++) {
-      gBh[g] = bp;
-      gBl[g] = bp + 2 * gP[g] * lda;
-      bp += 4 * gP[g] * lda;
-      gPart[g] = pp;
-      pp += N * gP[g] * gSplit[g];
-    }
+  // per side: two W buffers with their tensor maps (swizzled 32-column boxes
+  // for the update's left operand, unswizzled ones for the W' tile), two
+  // pivot-block inverses, the solve's right operand Bt (2P rows x lda, hi/lo)
+  // and its GEMM partials; the factor store (N rows x lda, L slices) is shared
+  struct Side {
+    float* W[2];
+    CUtensorMap mA[2], mWp[2], mBh, mBl;
+    float2* Tb;
+    float* bh;
+    float* bl;
+    float2* part;
+    int cur = 0;
+    int64_t gstep = 0;
+    cudaStream_t q = nullptr;
+    int64_t first = 0, count = 0, dir = 1;  // the side's slices: first, first + dir, ... (count of them)
+  } sd[2];
+  CUtensorMap mSh, mSl;
+  bool maps_ok = tc32::make_map(&mSh, st_hi, lda, N, L, lda, N * lda, tc32::BM) &&
+                 tc32::make_map(&mSl, st_lo, lda, N, L, lda, N * lda, tc32::BM);
+  for (int q = 0; q < nside; q++) {
+    Side& d = sd[q];
+    d.W[0] = static_cast<float*>(pW) + (2 * q) * N * lda;
+    d.W[1] = d.W[0] + N * lda;
+    d.Tb = static_cast<float2*>(pT) + 2 * q * NB * NB;
+    d.bh = bt_hi + q * 4 * P * lda;
+    d.bl = d.bh + 2 * P * lda;
+    d.part = static_cast<float2*>(pPart) + q * NP * sSplit;
+    for (int w = 0; w < 2; w++)
+      maps_ok = maps_ok && tc32::make_map(&d.mA[w], d.W[w], lda, N, 1, lda, 0, tc32::BM) &&
+                tc32::make_map(&d.mWp[w], d.W[w], lda, N, 1, lda, 0, tc32::BM, CU_TENSOR_MAP_SWIZZLE_NONE);
+    maps_ok = maps_ok && tc32::make_map(&d.mBh, d.bh, lda, 2 * P, 1, lda, 0, sbn) &&
+              tc32::make_map(&d.mBl, d.bl, lda, 2 * P, 1, lda, 0, sbn);
   }
-  bool maps_ok = true;
-  for (int g = 0; g < ngrp; g++)
-    maps_ok = maps_ok && tc32::make_map(&mBh[g], gBh[g], lda, 2 * gP[g], 1, lda, 0, sbn) &&
-              tc32::make_map(&mBl[g], gBl[g], lda, 2 * gP[g], 1, lda, 0, sbn);
-  if (!(tc32::make_map(&mA[0], Wb[0], lda, N, 1, lda, 0, tc32::BM) &&
-        tc32::make_map(&mA[1], Wb[1], lda, N, 1, lda, 0, tc32::BM) &&
-        tc32::make_map(&mWp[0], Wb[0], lda, N, 1, lda, 0, tc32::BM, CU_TENSOR_MAP_SWIZZLE_NONE) &&
-        tc32::make_map(&mWp[1], Wb[1], lda, N, 1, lda, 0, tc32::BM, CU_TENSOR_MAP_SWIZZLE_NONE) &&
-        tc32::make_map(&mSh, st_hi, lda, N, L, lda, N * lda, tc32::BM) &&
-        tc32::make_map(&mSl, st_lo, lda, N, L, lda, N * lda, tc32::BM) && maps_ok)) {
+  if (!maps_ok) {
     set_error("tensor-map encoding for the tcgen05 GEMM failed");
     return RGF_ERR_CUDA;
   }
+  sd[0].q = s;
+  sd[0].first = 0;
+  sd[0].count = two ? cj - 1 : L;
+  sd[0].dir = 1;
+  cudaStream_t s2 = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  struct StreamGuard {
+    cudaStream_t* st;
+    cudaEvent_t* f;
+    cudaEvent_t* j;
+    ~StreamGuard() {
+      if (*st) cudaStreamDestroy(*st);
+      if (*f) cudaEventDestroy(*f);
+      if (*j) cudaEventDestroy(*j);
+      t_use_pdl = true;
+    }
+  } sgd{&s2, &fork, &join};
+  if (two) {
+    RGF_CUDA_TRY_MX(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+    RGF_CUDA_TRY_MX(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+    RGF_CUDA_TRY_MX(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+    sd[1].q = s2;
+    sd[1].first = L - 1;
+    sd[1].count = L - cj;
+    sd[1].dir = -1;
+  }
+  auto fork_sides = [&]() -> rgf_status {
+    if (!two) return RGF_OK;
+    RGF_CUDA_TRY_MX(cudaEventRecord(fork, s));
+    RGF_CUDA_TRY_MX(cudaStreamWaitEvent(s2, fork, 0));
+    return RGF_OK;
+  };
+  auto join_sides = [&]() -> rgf_status {
+    if (!two) return RGF_OK;
+    RGF_CUDA_TRY_MX(cudaEventRecord(join, s2));
+    RGF_CUDA_TRY_MX(cudaStreamWaitEvent(s, join, 0));
+    return RGF_OK;
+  };
   RGF_CUDA_TRY_MX(cudaMemsetAsync(mstat, 0, sizeof(int), s));
-  RGF_CUDA_TRY_MX(cudaMemsetAsync(Wb[0], 0, 2 * sizeof(float) * N * lda, s));
-  RGF_CUDA_TRY_MX(cudaMemsetAsync(bt_hi, 0, 2 * sizeof(float) * 2 * P * lda, s));  // zero K padding of every group
+  RGF_CUDA_TRY_MX(cudaMemsetAsync(pW, 0, 2 * nside * sizeof(float) * N * lda, s));
+  RGF_CUDA_TRY_MX(cudaMemsetAsync(bt_hi, 0, 2 * nside * sizeof(float) * 2 * P * lda, s));  // zero K padding
   RGF_CUDA_TRY_MX(cudaMemsetAsync(x, 0, sizeof(double2) * NP * L, s));
   cudaEvent_t ev[3];
   for (int q = 0; q < 3; q++) RGF_CUDA_TRY_MX(cudaEventCreate(&ev[q]));
@@ -1001,61 +1063,103 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
     }
   } evg{ev};
   int64_t nl = 0;
+  t_use_pdl = !two;
 
   // (1) low-precision factorization
   RGF_CUDA_TRY_MX(cudaEventRecord(ev[0], s));
   const dim3 ga((unsigned)((ldw + 255) / 256), (unsigned)std::min<int64_t>(N, 8192));
   // one grid column more than the tiles: its first CTA serves the next pivot block
   const dim3 ggj((unsigned)((lda + gjs::BN - 1) / gjs::BN + 1), (unsigned)ntile_m);
-  const int64_t nsteps = (N + NB - 1) / NB;
-  int cur = 0;      // W buffer holding the current matrix
-  int64_t gstep = 0;  // steps issued so far (parity selects the pivot-block inverse buffer)
-  for (int64_t k = 0; k < L; k++) {
-    const double2* Ga = (k == 0) ? mp.G0[0] : nullptr;
-    const double2* Gb = (k == L - 1) ? mp.G0[1] : nullptr;
-    float* sh = k > 0 ? st_hi + (k - 1) * N * lda : st_hi;
-    float* sl = k > 0 ? st_lo + (k - 1) * N * lda : st_lo;
-    launch_pdl(k_mx_assemble, ga, dim3(256), 0, s, reinterpret_cast<float2*>(Wb[cur]), ldw, N, sh, sl, (int)(k > 0),
-               1, mp.st_col, mp.st_val, mp.k2, mp.eps + k * N, Ga, Gb);
+  auto lead = [&](int64_t k, int side) -> const double2* {  // lead block in slice k's matrix
+    if (side == 0) return (k == 0) ? mp.G0[0] : nullptr;
+    return (k == L - 1) ? mp.G0[1] : nullptr;
+  };
+  // slice k of side d: store the side's previous slice (kprev >= 0) and assemble
+  //   W = A_k - g_kprev - leads (- Wx at the junction)
+  auto assemble = [&](Side& d, int64_t k, int64_t kprev, const float2* Wx) {
+    float* sh = kprev >= 0 ? st_hi + kprev * N * lda : st_hi;
+    float* sl = kprev >= 0 ? st_lo + kprev * N * lda : st_lo;
+    launch_pdl(k_mx_assemble, ga, dim3(256), 0, d.q, reinterpret_cast<float2*>(d.W[d.cur]), ldw, N, sh, sl,
+               (int)(kprev >= 0), 1, mp.st_col, mp.st_val, mp.k2, mp.eps + k * N, lead(k, 0),
+               two ? lead(k, 1) : (k == L - 1 ? mp.G0[1] : nullptr), Wx);
     nl++;
-    if (k == 0) {
-      launch_pdl(k_mx_t0, dim3(1), dim3(256), 0, s, (const float*)Wb[cur], lda, (int)std::min<int64_t>(NB, N), Tbuf,
-                 mstat);
-      nl++;
+  };
+  auto store_only = [&](Side& d, int64_t k) {
+    launch_pdl(k_mx_assemble, ga, dim3(256), 0, d.q, reinterpret_cast<float2*>(d.W[d.cur]), ldw, N,
+               st_hi + k * N * lda, st_lo + k * N * lda, 1, 0, mp.st_col, mp.st_val, mp.k2, mp.eps,
+               (const double2*)nullptr, (const double2*)nullptr, (const float2*)nullptr);
+    nl++;
+  };
+  auto first_t = [&](Side& d) {
+    launch_pdl(k_mx_t0, dim3(1), dim3(256), 0, d.q, (const float*)d.W[d.cur], lda, (int)std::min<int64_t>(NB, N),
+               d.Tb + (d.gstep & 1) * NB * NB, mstat);
+    nl++;
+  };
+  // one Gauss-Jordan step of side d's slice k; knext: the slice whose first
+  // pivot block the server prepares after the last step (< 0: none)
+  auto gj_step = [&](Side& d, int64_t j0, int64_t knext) {
+    const int jn = (int)std::min<int64_t>(NB, N - j0);
+    GjNext ns{};
+    ns.Tin = d.Tb + (d.gstep & 1) * NB * NB;
+    ns.Tout = d.Tb + ((d.gstep + 1) & 1) * NB * NB;
+    ns.st_col = mp.st_col;
+    ns.st_val = mp.st_val;
+    ns.k2 = mp.k2;
+    ns.ldg = N;
+    if (j0 + NB < N) {
+      ns.j1 = (int)(j0 + NB);
+      ns.jn1 = (int)std::min<int64_t>(NB, N - j0 - NB);
+    } else if (knext >= 0) {  // the next slice's first block
+      ns.j1 = 0;
+      ns.jn1 = (int)std::min<int64_t>(NB, N);
+      ns.next_slice = 1;
+      ns.same_block = N <= NB;
+      ns.eps_next = mp.eps + knext * N;
+      ns.g0r = (knext == L - 1) ? mp.G0[1] : (knext == 0 ? mp.G0[0] : nullptr);
+    } else {
+      ns.Tout = nullptr;  // nothing follows this step within the side
     }
-    for (int64_t j0 = 0; j0 < N; j0 += NB) {
-      const int jn = (int)std::min<int64_t>(NB, N - j0);
-      GjNext ns{};
-      ns.Tin = Tbuf + (gstep & 1) * NB * NB;
-      ns.Tout = Tbuf + ((gstep + 1) & 1) * NB * NB;
-      ns.st_col = mp.st_col;
-      ns.st_val = mp.st_val;
-      ns.k2 = mp.k2;
-      ns.ldg = N;
-      if (j0 + NB < N) {
-        ns.j1 = (int)(j0 + NB);
-        ns.jn1 = (int)std::min<int64_t>(NB, N - j0 - NB);
-      } else if (k + 1 < L) {  // the next slice's first block
-        ns.j1 = 0;
-        ns.jn1 = (int)std::min<int64_t>(NB, N);
-        ns.next_slice = 1;
-        ns.same_block = nsteps == 1;
-        ns.eps_next = mp.eps + (k + 1) * N;
-        ns.g0r = (k + 1 == L - 1) ? mp.G0[1] : nullptr;
-      } else {
-        ns.Tout = nullptr;  // the last step of the last slice: nothing follows
+    launch_pdl(k_mx_gj_step, ggj, dim3(256), gjs::SMEM, d.q, d.mA[d.cur], d.mWp[d.cur], (const float*)d.W[d.cur],
+               d.W[d.cur ^ 1], lda, (int)N, (int)j0, jn, ns, mstat, kGemmTimeout);
+    d.cur ^= 1;
+    d.gstep++;
+    nl++;
+  };
+  if ((st = fork_sides())) return st;
+  const int64_t nmax = std::max(sd[0].count, two ? sd[1].count : 0);
+  for (int64_t i = 0; i < nmax; i++) {
+    for (int q = 0; q < nside; q++) {
+      Side& d = sd[q];
+      if (i >= d.count) continue;
+      const int64_t k = d.first + d.dir * i;
+      assemble(d, k, i > 0 ? k - d.dir : -1, nullptr);
+      if (i == 0) first_t(d);
+    }
+    for (int64_t j0 = 0; j0 < N; j0 += NB)
+      for (int q = 0; q < nside; q++) {
+        Side& d = sd[q];
+        if (i >= d.count) continue;
+        const int64_t k = d.first + d.dir * i;
+        gj_step(d, j0, i + 1 < d.count ? k + d.dir : -1);
       }
-      launch_pdl(k_mx_gj_step, ggj, dim3(256), gjs::SMEM, s, mA[cur], mWp[cur], (const float*)Wb[cur],
-                 Wb[cur ^ 1], lda, (int)N, (int)j0, jn, ns, mstat, kGemmTimeout);
-      cur ^= 1;
-      gstep++;
-      nl++;
-    }
   }
-  launch_pdl(k_mx_assemble, ga, dim3(256), 0, s, reinterpret_cast<float2*>(Wb[cur]), ldw, N,
-             st_hi + (L - 1) * N * lda, st_lo + (L - 1) * N * lda, 1, 0, mp.st_col, mp.st_val, mp.k2, mp.eps,
-             (const double2*)nullptr, (const double2*)nullptr);
-  nl++;
+  if ((st = join_sides())) return st;
+  t_use_pdl = true;
+  if (two) {
+    // the right side's last slice (cj) into the store, then the junction slice
+    // cj - 1 = A - g_{cj-2} (left side's W) - g_{cj} (right side's W)
+    Side& dl = sd[0];
+    Side& dr = sd[1];
+    dr.q = s;
+    store_only(dr, cj);
+    assemble(dl, cj - 1, cj - 2, reinterpret_cast<const float2*>(dr.W[dr.cur]));
+    first_t(dl);
+    for (int64_t j0 = 0; j0 < N; j0 += NB) gj_step(dl, j0, -1);
+    store_only(dl, cj - 1);
+    dr.q = s2;
+  } else {
+    store_only(sd[0], L - 1);
+  }
   RGF_CUDA_TRY_MX(cudaGetLastError());
   RGF_CUDA_TRY_MX(cudaEventRecord(ev[1], s));
 
@@ -1069,48 +1173,43 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
 
   // (3) refinement
   tc32::GemmArgs gs[2];
-  dim3 gsg[2], gp[2];
-  cudaStream_t gst[2] = {s, nullptr};
-  cudaEvent_t fork = nullptr, join = nullptr;
-  struct StreamGuard {
-    cudaStream_t* st;
-    cudaEvent_t* f;
-    cudaEvent_t* j;
-    ~StreamGuard() {
-      if (*st) cudaStreamDestroy(*st);
-      if (*f) cudaEventDestroy(*f);
-      if (*j) cudaEventDestroy(*j);
-    }
-  } sg{&gst[1], &fork, &join};
-  if (ngrp == 2) {
-    RGF_CUDA_TRY_MX(cudaStreamCreateWithFlags(&gst[1], cudaStreamNonBlocking));
-    RGF_CUDA_TRY_MX(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
-    RGF_CUDA_TRY_MX(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+  for (int q = 0; q < nside; q++) {
+    gs[q] = tc32::GemmArgs{};
+    gs[q].M = (int)N;
+    gs[q].Nr = (int)(2 * P);
+    gs[q].k_chunks = kchunks / sSplit;
+    gs[q].mode = tc32::kPartial;
+    gs[q].out = reinterpret_cast<float*>(sd[q].part);
+    gs[q].ldo = 2 * P;
+    gs[q].split_stride = 2 * NP;
+    gs[q].err = mstat;
+    gs[q].timeout = kGemmTimeout;
   }
-  for (int g = 0; g < ngrp; g++) {
-    gs[g] = tc32::GemmArgs{};
-    gs[g].M = (int)N;
-    gs[g].Nr = (int)(2 * gP[g]);
-    gs[g].k_chunks = kchunks / gSplit[g];
-    gs[g].mode = tc32::kPartial;
-    gs[g].out = reinterpret_cast<float*>(gPart[g]);
-    gs[g].ldo = 2 * gP[g];
-    gs[g].split_stride = 2 * N * gP[g];
-    gs[g].err = mstat;
-    gs[g].timeout = kGemmTimeout;
-    gsg[g] = dim3((unsigned)gTiles[g], (unsigned)ntile_m, (unsigned)gSplit[g]);
-    gp[g] = dim3((unsigned)((gP[g] + 31) / 32), (unsigned)((N + 31) / 32));
-  }
+  const dim3 gsg((unsigned)sTiles, (unsigned)ntile_m, (unsigned)sSplit);
+  const dim3 gp((unsigned)((P + 31) / 32), (unsigned)((N + 31) / 32));
   const dim3 tp(32, 8);
-  auto gemm = [&](int g, int64_t k) {
-    gs[g].a_z = (int)k;
-    cudaStream_t q = gst[g];
+  // side q's GEMM: partials = g_k Bt (Bt of side qb, default q)
+  auto gemm = [&](int q, int64_t k, cudaStream_t qs) {
+    gs[q].a_z = (int)k;
     if (sbn == 64)
-      launch_pdl(tc32::k_tc32_gemm<64>, gsg[g], dim3(tc32::kThreads), tc32::Cfg<64>::SMEM, q, mSh, mSl, mBh[g],
-                 mBl[g], gs[g]);
+      launch_pdl(tc32::k_tc32_gemm<64>, gsg, dim3(tc32::kThreads), tc32::Cfg<64>::SMEM, qs, mSh, mSl, sd[q].mBh,
+                 sd[q].mBl, gs[q]);
     else
-      launch_pdl(tc32::k_tc32_gemm<128>, gsg[g], dim3(tc32::kThreads), tc32::Cfg<128>::SMEM, q, mSh, mSl, mBh[g],
-                 mBl[g], gs[g]);
+      launch_pdl(tc32::k_tc32_gemm<128>, gsg, dim3(tc32::kThreads), tc32::Cfg<128>::SMEM, qs, mSh, mSl, sd[q].mBh,
+                 sd[q].mBl, gs[q]);
+    nl++;
+  };
+  auto fwd_prep = [&](int q, int64_t k, int64_t kprev, cudaStream_t qs, int q2 = -1, int64_t kprev2 = -1) {
+    launch_pdl(k_mx_fwd_prep, gp, tp, 0, qs, k, kprev, N, P, P, (int64_t)0, y, (const float2*)sd[q].part, sSplit,
+               (const float2*)(q2 >= 0 ? sd[q2].part : nullptr), kprev2, sSplit, sd[q].bh, sd[q].bl, lda,
+               (const int*)nullptr);
+    nl++;
+  };
+  auto bwd_prep = [&](int q, int64_t k, int add_y, int write_bt, cudaStream_t qs, int q2 = -1) {
+    launch_pdl(k_mx_bwd_prep, gp, tp, 0, qs, k, L, N, P, P, (int64_t)0, x, (const float2*)y,
+               (const float2*)sd[q].part, sSplit, sd[q].bh, sd[q].bl, lda, norms, (const int*)nullptr, add_y,
+               write_bt, q2 >= 0 ? sd[q2].bh : nullptr, q2 >= 0 ? sd[q2].bl : nullptr);
+    nl++;
   };
   double prev = 1.0, change = 1.0;
   bool conv = false;
@@ -1128,32 +1227,46 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
                (const double2*)b0, (const double2*)bL, (const double2*)(have_x ? e0 : nullptr),
                (const double2*)(have_x ? e1 : nullptr));
     nl++;
-    if (ngrp == 2) {
-      RGF_CUDA_TRY_MX(cudaEventRecord(fork, s));
-      RGF_CUDA_TRY_MX(cudaStreamWaitEvent(gst[1], fork, 0));
-    }
-    // forward then backward substitution; the column groups' launches
-    // interleaved slice by slice so that both streams are fed
-    for (int64_t k = 0; k < L; k++)
-      for (int g = 0; g < ngrp; g++) {
-        launch_pdl(k_mx_fwd_prep, gp[g], tp, 0, gst[g], k, N, gP[g], P, gOff[g], y, (const float2*)gPart[g],
-                   gSplit[g], gBh[g], gBl[g], lda);
-        gemm(g, k);
-        nl += 2;
+    if (!two) {
+      // forward y_k = g_k (r_k + y_{k-1}), backward d_k = y_k + g_k d_{k+1}
+      for (int64_t k = 0; k < L; k++) {
+        fwd_prep(0, k, k - 1, s);
+        gemm(0, k, s);
       }
-    for (int64_t k = L - 1; k >= 0; k--)
-      for (int g = 0; g < ngrp; g++) {
-        launch_pdl(k_mx_bwd_prep, gp[g], tp, 0, gst[g], k, L, N, gP[g], P, gOff[g], x, (const float2*)y,
-                   (const float2*)gPart[g], gSplit[g], gBh[g], gBl[g], lda, norms);
-        nl++;
-        if (k > 0) {
-          gemm(g, k - 1);
-          nl++;
+      for (int64_t k = L - 1; k >= 0; k--) {
+        bwd_prep(0, k, k < L - 1, k > 0, s);
+        if (k > 0) gemm(0, k - 1, s);
+      }
+    } else {
+      // forward from both leads towards the junction slice cj - 1
+      if ((st = fork_sides())) return st;
+      t_use_pdl = false;
+      const int64_t nmx = std::max(sd[0].count, sd[1].count);
+      for (int64_t i = 0; i < nmx; i++)
+        for (int q = 0; q < 2; q++) {
+          if (i >= sd[q].count) continue;
+          const int64_t k = sd[q].first + sd[q].dir * i;
+          fwd_prep(q, k, i > 0 ? k - sd[q].dir : -1, sd[q].q);
+          gemm(q, k, sd[q].q);
         }
-      }
-    if (ngrp == 2) {
-      RGF_CUDA_TRY_MX(cudaEventRecord(join, gst[1]));
-      RGF_CUDA_TRY_MX(cudaStreamWaitEvent(s, join, 0));
+      if ((st = join_sides())) return st;
+      t_use_pdl = true;
+      // junction: d_{cj-1} = G_{cj-1} (r + y_{cj-2} + y_{cj}), into both sides' Bt
+      fwd_prep(0, cj - 1, cj - 2, s, 1, cj);
+      gemm(0, cj - 1, s);
+      bwd_prep(0, cj - 1, 0, 1, s, 1);
+      // backward outwards: d_k = y_k + g_k d_{k +- 1}
+      if ((st = fork_sides())) return st;
+      t_use_pdl = false;
+      for (int64_t i = nmx - 1; i >= 0; i--)
+        for (int q = 0; q < 2; q++) {
+          if (i >= sd[q].count) continue;
+          const int64_t k = sd[q].first + sd[q].dir * i;
+          gemm(q, k, sd[q].q);
+          bwd_prep(q, k, 1, i > 0, sd[q].q);
+        }
+      if ((st = join_sides())) return st;
+      t_use_pdl = true;
     }
     RGF_CUDA_TRY_MX(cudaGetLastError());
     double hn[8];

@@ -59,6 +59,7 @@ struct GemmArgs {
   int gj_c0, gj_nb;        // kGJ: pivot block (complex columns)
   int* err;                // error word (kErrTimeout)
   long long timeout;       // spin limit in SM clock cycles
+  const int* az_dev;       // non-null: a_z is added to *az_dev (read after the grid before has finished)
 };
 
 template <int BN>
@@ -172,6 +173,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
   const int kc0 = blockIdx.z * g.k_chunks;
+  int a_z = g.a_z;
   auto sA_hi = [&](int s) { return base + (uint32_t)s * C::STAGE_BYTES; };
   auto sA_lo = [&](int s) { return sA_hi(s) + C::A_BYTES; };
   auto sB_hi = [&](int s) { return sA_hi(s) + 2 * C::A_BYTES; };
@@ -198,6 +200,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = tmem_sh;
   asm volatile("griddepcontrol.wait;" ::: "memory");  // the operands and `out` of the grid before
+  if (g.az_dev) a_z += *g.az_dev;
 
   if (warp == 0 && lane == 0) {
     // producer: one stage = A_hi, A_lo (BM rows) and B_hi, B_lo (BN rows) of BK floats
@@ -211,8 +214,8 @@ __global__ void __launch_bounds__(kThreads, 1)
       asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(fb), "r"(C::STAGE_BYTES)
                    : "memory");
       const int kx = (kc0 + kt) * BK;
-      tma_load_3d(sA_hi(s), &ta_hi, kx, m0, g.a_z, fb);
-      tma_load_3d(sA_lo(s), &ta_lo, kx, m0, g.a_z, fb);
+      tma_load_3d(sA_hi(s), &ta_hi, kx, m0, a_z, fb);
+      tma_load_3d(sA_lo(s), &ta_lo, kx, m0, a_z, fb);
       tma_load_3d(sB_hi(s), &tb_hi, kx, n0, g.b_z, fb);
       tma_load_3d(sB_lo(s), &tb_lo, kx, n0, g.b_z, fb);
     }
