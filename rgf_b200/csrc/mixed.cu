@@ -81,10 +81,6 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;"
 
 // launch with programmatic stream serialization (every kernel launched this
 // way waits for its predecessor with pdl_wait before it reads or writes)
-// off while two streams run the two sides at once: a stream's early-launched,
-// waiting CTAs would hold SMs that the other stream's kernels need
-thread_local bool t_use_pdl = true;
-
 template <typename... KArgs, typename... Args>
 cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
                        Args&&... args) {
@@ -97,7 +93,7 @@ cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t sme
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
-  cfg.numAttrs = t_use_pdl ? 1 : 0;
+  cfg.numAttrs = 1;
   return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
 }
 
@@ -1026,7 +1022,6 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
       if (*st) cudaStreamDestroy(*st);
       if (*f) cudaEventDestroy(*f);
       if (*j) cudaEventDestroy(*j);
-      t_use_pdl = true;
     }
   } sgd{&s2, &fork, &join};
   if (two) {
@@ -1063,7 +1058,6 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
     }
   } evg{ev};
   int64_t nl = 0;
-  t_use_pdl = !two;
 
   // (1) low-precision factorization
   RGF_CUDA_TRY_MX(cudaEventRecord(ev[0], s));
@@ -1144,7 +1138,6 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
       }
   }
   if ((st = join_sides())) return st;
-  t_use_pdl = true;
   if (two) {
     // the right side's last slice (cj) into the store, then the junction slice
     // cj - 1 = A - g_{cj-2} (left side's W) - g_{cj} (right side's W)
@@ -1240,7 +1233,6 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
     } else {
       // forward from both leads towards the junction slice cj - 1
       if ((st = fork_sides())) return st;
-      t_use_pdl = false;
       const int64_t nmx = std::max(sd[0].count, sd[1].count);
       for (int64_t i = 0; i < nmx; i++)
         for (int q = 0; q < 2; q++) {
@@ -1250,14 +1242,12 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
           gemm(q, k, sd[q].q);
         }
       if ((st = join_sides())) return st;
-      t_use_pdl = true;
       // junction: d_{cj-1} = G_{cj-1} (r + y_{cj-2} + y_{cj}), into both sides' Bt
       fwd_prep(0, cj - 1, cj - 2, s, 1, cj);
       gemm(0, cj - 1, s);
       bwd_prep(0, cj - 1, 0, 1, s, 1);
       // backward outwards: d_k = y_k + g_k d_{k +- 1}
       if ((st = fork_sides())) return st;
-      t_use_pdl = false;
       for (int64_t i = nmx - 1; i >= 0; i--)
         for (int q = 0; q < 2; q++) {
           if (i >= sd[q].count) continue;
@@ -1266,7 +1256,6 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
           bwd_prep(q, k, 1, i > 0, sd[q].q);
         }
       if ((st = join_sides())) return st;
-      t_use_pdl = true;
     }
     RGF_CUDA_TRY_MX(cudaGetLastError());
     double hn[8];

@@ -100,3 +100,29 @@ def test_unsupported_combinations(handle):
     T0, _ = rgf_b200.cal_smatrix_RGF(case["syst"], ["right"], ["left"], handle=handle)
     with pytest.raises(_abi.RGFError):
         rgf_b200.smatrix_grad_RGF(case["syst"], ["right"], ["left"], np.conj(T0), options=OPT, handle=handle)
+
+
+@pytest.mark.parametrize("ny,nx,bc", [(40, 7, "periodic"), (40, 8, "Dirichlet"), (70, 9, "Neumann"),
+                                      (96, 16, 0.4), (33, 17, "DirichletNeumann"), (130, 64, "periodic")])
+def test_two_sided_edges(ny, nx, bc, handle):
+    """One chain below 8 slices, the two-sided factorization from 8 on (odd and
+    even L: sides of equal or unequal length), N not a multiple of the 32-wide
+    pivot block; against the FP64 form of the same call."""
+    rng = np.random.default_rng(ny * 100 + nx)
+    syst = dict(epsilon=1 + 2 * rng.random((ny, nx)) + 0.01j * rng.random((ny, nx)), epsilon_L=1.0,
+                epsilon_R=1.5, k0dx=2 * np.pi / 12, yBC=bc)
+    S64, _ = rgf_b200.cal_smatrix_RGF(syst, ["left", "right"], ["left", "right"], handle=handle)
+    S, _ = rgf_b200.cal_smatrix_RGF(syst, ["left", "right"], ["left", "right"], options=OPT, handle=handle)
+    info = handle.refinement()
+    assert info["form"] == _abi.RGF_TF32X3, info
+    assert rel(S, S64) <= TOL_S, (rel(S, S64), info)
+
+
+def test_two_sided_3d(handle):
+    rng = np.random.default_rng(9)
+    eps = np.where(rng.random((8, 6, 21)) < 0.4, 2.25, 1.0)
+    syst = dict(epsilon=eps, epsilon_L=1.0, epsilon_R=1.0, k0dx=2 * np.pi / 10, xyBC="periodic")
+    S64, _ = rgf_b200.cal_smatrix_RGF_3D(syst, ["left", "right"], ["left", "right"], handle=handle)
+    S, _ = rgf_b200.cal_smatrix_RGF_3D(syst, ["left", "right"], ["left", "right"], options=OPT, handle=handle)
+    assert handle.refinement()["form"] == _abi.RGF_TF32X3
+    assert rel(S, S64) <= TOL_S
