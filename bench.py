@@ -20,6 +20,10 @@ A step is one full S-matrix (204 x 204) of the config-2 structure.
 * cpu_baseline: the numpy/scipy oracle (restatement of the MATLAB reference;
            MATLAB itself is not installed) on the host cores, on a bounded
            sample of slices, extrapolated linearly in L.
+* precision_form: the split-precision form (RGF_TF32X3: FP32 factorization
+           with 3xTF32 tcgen05 updates + FP64 refinement) on the same
+           structure, timed like `value`, with its ratio to `value` and its
+           error against the oracle; config 3 (3D) beside it.
 * --impl reference: that CPU oracle timed alone, same metric and config.
 
 Multi-GPU (torchrun): replicas only -- each rank computes its own S-matrices;
@@ -304,8 +308,11 @@ def precision_form(step, read_S, S_fp64, h, flush, stream, fp64_value, gpath, de
            "refinement_passes": info["iterations"], "last_correction": info["last_change"],
            "factor_ms": info["factor_ms"], "solve_ms": info["solve_ms"],
            "rel_err_vs_fp64_this_run": float(np.linalg.norm(Sp - S_fp64) / np.linalg.norm(S_fp64)),
+           "effective_tflops": None,
            "workload": "config2 (as value)",
            "compared_with": "the FP64 plain form of this line (persistent FP64 DMMA sweep)"}
+    # canonical flops of the FP64 form's recursion (the work either form stands in for)
+    out["effective_tflops"] = workloads.canonical_flops(1024, 4096, 102, 102) * v / 1e12
     if os.path.exists(gpath):
         S0 = np.load(gpath, allow_pickle=True)["S"]
         out["rel_err_vs_oracle"] = float(np.linalg.norm(Sp - S0) / np.linalg.norm(S0))
