@@ -332,7 +332,7 @@ def precision_form(step, read_S, S_fp64, h, flush, stream, fp64_value, gpath, de
     return out
 
 
-def batch_rate(dev, count: int = 256, workers: int = 0):
+def batch_rate(dev, count: int = 256, workers: int = 0, precision: int = 0):
     """Config-4 batched form: all 256 seeded structures (N uniform 64..512,
     L uniform 100..2000, eps 1+2U, complex k0dx), full S each, through
     rgf_smatrix_batch_2d with host inputs and outputs (workers = 0: every
@@ -345,12 +345,14 @@ def batch_rate(dev, count: int = 256, workers: int = 0):
     systs = [it[0] for it in items]
     outs = [it[1] for it in items]
     ins = [it[2] for it in items]
-    rgf_b200.cal_smatrix_RGF_batch(systs[:4], outs[:4], ins[:4], workers=workers, device=dev)
+    opt = {"precision": precision}
+    rgf_b200.cal_smatrix_RGF_batch(systs[:4], outs[:4], ins[:4], workers=workers, device=dev, options=opt)
     t0 = time.perf_counter()
-    rgf_b200.cal_smatrix_RGF_batch(systs, outs, ins, workers=workers, device=dev)
+    rgf_b200.cal_smatrix_RGF_batch(systs, outs, ins, workers=workers, device=dev, options=opt)
     dt = time.perf_counter() - t0
     Ns, Ls, _ = workloads.config4_params()
     return {"value": count / dt, "unit": "S-matrices/s", "structures": count, "workers": workers,
+            "form": "split precision (RGF_TF32X3)" if precision else "FP64",
             "seconds": dt, "sum_L_N3": float(np.sum(Ls[:count].astype(float) * Ns[:count].astype(float) ** 3)),
             "workload": "config4: the 256-structure batch (N U{64..512}, L U{100..2000}, "
                         "eps 1+2U, k0dx = 2pi/15 (1 + i eta), eta U[0,1e-3), periodic, full S)",
@@ -460,6 +462,7 @@ def run_ours(args, dist):
     line["grad_over_fwd"] = grad_over_fwd(h, dev, stream) if not args.slices else None
     line["batch"] = batch_rate(dev, workers=0) if not args.slices else None
     line["batch_pipelines"] = batch_rate(dev, workers=16) if not args.slices else None
+    line["batch_split_precision"] = batch_rate(dev, workers=8, precision=1) if not args.slices else None
     n, ms, fl_exec, name = prof
     fl = nx * workloads.canonical_slice_flops(ny, n_in // 2, n_out // 2)  # the launch covers all nx slices
     achieved = fl / (ms / n / 1e3) / 1e12 if n else None

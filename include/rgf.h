@@ -174,7 +174,9 @@ RGF_API rgf_status rgf_smatrix_3d(rgf_handle h, const rgf_syst3d* syst, const rg
  * needs tiles smaller than 96 x 96 sweeps on its own first).  workers > 0:
  * that many concurrent pipelines (host threads, each with its own stream and
  * workspace), whose persistent sweeps share the GPU's SMs through one budget.
- * statuses (may be NULL) receives each problem's status; the return value
+ * With opt->precision = RGF_TF32X3 every structure takes the split-precision
+ * form, as pipelines (workers <= 0: 8; each pipeline holds its structure's
+ * factor store, 8 N lda L bytes).  statuses (may be NULL) receives each problem's status; the return value
  * is the first failure (message names the item).  The reference has no
  * batched call: its user loops over cal_smatrix_RGF. */
 RGF_API rgf_status rgf_smatrix_batch_2d(rgf_handle h, int64_t count, const rgf_syst2d* systs,

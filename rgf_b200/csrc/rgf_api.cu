@@ -1565,8 +1565,11 @@ rgf_status rgf_smatrix_batch_2d(rgf_handle h, int64_t count, const rgf_syst2d* s
     return RGF_ERR_ARG;
   }
   RGF_CUDA_TRY(cudaSetDevice(h->device));
-  if (workers <= 0) return batch_one_launch(h, count, systs, reqs, opt, S, ldS, statuses);
-  int nw = workers;
+  // the split-precision form runs as pipelines (8 by default: each holds its
+  // structure's factor store, up to ~12 GB for N = 512, L = 2000)
+  const bool split = opt && opt->precision == RGF_TF32X3;
+  if (workers <= 0 && !split) return batch_one_launch(h, count, systs, reqs, opt, S, ldS, statuses);
+  int nw = workers > 0 ? workers : 8;
   nw = (int)std::min<int64_t>(nw, count);
   nw = std::max(1, std::min(nw, h->sms / 2));
   RGF_CUDA_TRY(cudaSetDevice(h->device));

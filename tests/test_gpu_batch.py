@@ -82,3 +82,25 @@ def test_one_launch_batch_runs_one_gang_launch():
     for s, o, i, S in zip(systs, outs, ins, Sb):
         S1, _ = rgf_b200.cal_smatrix_RGF(s, o, i)
         assert rel(S, S1) <= 1e-12
+
+
+@pytest.mark.parametrize("workers", [0, 3])
+def test_batch_split_precision(workers):
+    """The batched entry with the split-precision form: config-4 structures
+    against the oracle fixtures at the form's 1e-10, and the mixed batch
+    against single FP64 calls."""
+    names = ["cfg4_0", "cfg4_7", "cfg4_9"]
+    cases = [config_case(n) for n in names]
+    cases = [c for c in cases if c is not None]
+    opt = {"precision": _abi.RGF_TF32X3}
+    Sb = rgf_b200.cal_smatrix_RGF_batch([c["syst"] for c in cases], [c["out"] for c in cases],
+                                        [c["in"] for c in cases], workers=workers, options=opt)
+    for c, S in zip(cases, Sb):
+        assert rel(S, c["S"]) <= 1e-10, c["name"]
+    systs, outs, ins = mixed_batch(n=6, seed=41)
+    Sb = rgf_b200.cal_smatrix_RGF_batch(systs, outs, ins, workers=workers, options=opt)
+    for s, o, i, S in zip(systs, outs, ins, Sb):
+        S1, _ = rgf_b200.cal_smatrix_RGF(s, o, i)
+        assert S.shape == S1.shape
+        if S1.size:
+            assert rel(S, S1) <= 1e-10
