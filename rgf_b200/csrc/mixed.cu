@@ -751,14 +751,17 @@ __global__ void __launch_bounds__(256, 1)
     float2 acc[8];
 #pragma unroll
     for (int v = 0; v < 8; v++) acc[v] = make_float2(0.f, 0.f);
-#pragma unroll 4
+    const float4* Wj4 = reinterpret_cast<const float4*>(Wj) + warp * 4;  // 8 complex = 4 float4 per row
+#pragma unroll 8
     for (int sr = 0; sr < NB; sr++) {
       const float2 tv = Ts[lane * (NB + 1) + sr];
 #pragma unroll
-      for (int v = 0; v < 8; v++) {
-        const float2 w = Wj[sr * 64 + warp * 8 + v];
-        acc[v].x += tv.x * w.x - tv.y * w.y;
-        acc[v].y += tv.x * w.y + tv.y * w.x;
+      for (int v2 = 0; v2 < 4; v2++) {
+        const float4 w = Wj4[sr * 32 + v2];  // broadcast: every lane reads the same row of W'(J, :)
+        acc[2 * v2].x = fmaf(tv.x, w.x, fmaf(-tv.y, w.y, acc[2 * v2].x));
+        acc[2 * v2].y = fmaf(tv.x, w.y, fmaf(tv.y, w.x, acc[2 * v2].y));
+        acc[2 * v2 + 1].x = fmaf(tv.x, w.z, fmaf(-tv.y, w.w, acc[2 * v2 + 1].x));
+        acc[2 * v2 + 1].y = fmaf(tv.x, w.w, fmaf(tv.y, w.z, acc[2 * v2 + 1].y));
       }
     }
     const int kf = 2 * lane, kc = kf >> 5, kk = kf & 31, gq = kk >> 2, ofs = (kk & 3) * 4;
