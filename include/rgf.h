@@ -79,7 +79,8 @@ typedef enum {
                     tensor-core updates (tcgen05), S won back by FP64 iterative
                     refinement of the block-tridiagonal solve against the FP64
                     operator; falls back to RGF_FP64 when the refinement does not
-                    converge (rgf_last_refinement tells).  S-matrices only
+                    converge or its factor store (8 N lda L bytes, lda = 2N
+                    rounded up to 32) does not fit (rgf_last_refinement tells).  S-matrices only
                     (rgf_smatrix_2d/3d and the pipelined batch).              */
 } rgf_precision;
 

@@ -760,7 +760,18 @@ rgf_status smatrix_run(rgf_handle h, const Problem& p, const rgf_request* req, c
       h->mx_form = RGF_TF32X3;
       return copy_channels_out(h, tr, ci, ch);
     }
-    if (st != kMixedNotConverged) return st;
+    if (st == RGF_ERR_OOM) {
+      // the factor store does not fit: give its buffers back and take the
+      // FP64 form, which needs a small fraction of the memory
+      cudaGetLastError();
+      for (DevBuf& b : h->mx) {
+        if (b.p) cudaFreeAsync(b.p, h->stream);
+        b.p = nullptr;
+        b.bytes = 0;
+      }
+    } else if (st != kMixedNotConverged) {
+      return st;
+    }
     h->mx_fallback = 1;  // S from the FP64 form
   }
 
