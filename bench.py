@@ -225,6 +225,20 @@ def measure_fp64_peak(device: int):
     return FP64_DMMA_FALLBACK_TFLOPS, "fallback: earlier FP64 DMMA measurement on this pool (37 TFLOP/s)"
 
 
+def measure_tf32_peak(device: int):
+    """Dense TF32 tensor-core rate of tcgen05.mma kind::tf32 measured now on
+    this GPU (librgf_peak.so), TFLOP/s, or None."""
+    from rgf_b200 import build
+    try:
+        lib = ctypes.CDLL(str(build.PEAK_OUT))
+        out = ctypes.c_double(0.0)
+        if lib.rgf_peak_tf32(ctypes.c_int(device), ctypes.byref(out)) == 0 and out.value > 0:
+            return out.value
+    except (OSError, AttributeError):
+        pass
+    return None
+
+
 def grad_over_fwd(h, dev, stream, reps: int = 5):
     """Config-5 adjoint cost: time of rgf_smatrix_grad_2d (S and dF/d eps for
     F = sum |t_ab|^2 over 8 left inputs -> 8 right outputs, checkpoint every 23
@@ -311,8 +325,12 @@ def precision_form(step, read_S, S_fp64, h, flush, stream, fp64_value, gpath, de
            "effective_tflops": None,
            "workload": "config2 (as value)",
            "compared_with": "the FP64 plain form of this line (persistent FP64 DMMA sweep)"}
-    # canonical flops of the FP64 form's recursion (the work either form stands in for)
+    # canonical flops of the FP64 form's recursion (the work either form stands in for),
+    # against a third of the TF32 tensor rate measured now (3 TF32 products per product)
     out["effective_tflops"] = workloads.canonical_flops(1024, 4096, 102, 102) * v / 1e12
+    tf32 = measure_tf32_peak(dev)
+    out["tf32_peak_tflops"] = tf32
+    out["frac_of_3xtf32_peak"] = out["effective_tflops"] / (tf32 / 3) if tf32 else None
     if os.path.exists(gpath):
         S0 = np.load(gpath, allow_pickle=True)["S"]
         out["rel_err_vs_oracle"] = float(np.linalg.norm(Sp - S0) / np.linalg.norm(S0))

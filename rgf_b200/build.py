@@ -68,10 +68,12 @@ def build(verbose: bool = False, force: bool = False) -> Path:
 
 def build_peak(verbose: bool = False, force: bool = False) -> Path:
     src = CSRC / "peak.cu"
-    if PEAK_OUT.exists() and not force and PEAK_OUT.stat().st_mtime >= src.stat().st_mtime:
+    if PEAK_OUT.exists() and not force and PEAK_OUT.stat().st_mtime >= max(src.stat().st_mtime,
+                                                                            (CSRC / "tc32.cuh").stat().st_mtime):
         return PEAK_OUT
     tmp = PEAK_OUT.with_suffix(".so.tmp")
-    cmd = [nvcc(), *ARCH, *FLAGS, "-shared", "-cudart", "static", "-o", str(tmp), str(src)]
+    cmd = [nvcc(), *ARCH, *FLAGS, "-I", str(PKG.parent / "include"), "-shared", "-cudart", "static", "-o", str(tmp),
+           str(src)]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)

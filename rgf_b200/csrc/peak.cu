@@ -10,7 +10,56 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "tc32.cuh"
+
 namespace {
+
+// TF32 tensor-core peak: one CTA per SM issues back-to-back
+// tcgen05.mma.cta_group::1.kind::tf32 of M = 128, N = 256, K = 8 from
+// operands resident in shared memory into a TMEM accumulator (the shape the
+// 3xTF32 GEMMs of the split-precision form issue), one commit at the end.
+constexpr uint32_t kPkA = 128 * 32 * 4, kPkB = 256 * 32 * 4;
+__global__ void __launch_bounds__(128, 1) k_tf32_peak(int iters, int* err) {
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t done;
+  __shared__ uint32_t tmem_sh;
+  using namespace rgf::tc32;
+  const uint32_t base = (su32(smem_raw) + 1023u) & ~1023u;
+  float* f = reinterpret_cast<float*>(smem_raw + (base - su32(smem_raw)));
+  for (int i = threadIdx.x; i < (int)((kPkA + kPkB) / 4); i += blockDim.x) f[i] = 1.0f / (1 + (i & 63));
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    mbar_init(su32(&done), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tmem_sh)), "r"(256)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = tmem_sh;
+  GemmArgs g{};
+  g.err = err;
+  g.timeout = 20000000000LL;
+  if (warp == 1 && lane == 0) {
+    constexpr uint32_t idesc =
+        (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(256 >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+    const uint64_t da = sw128_desc(base), db = sw128_desc(base + kPkA);
+    for (int it = 0; it < iters; it++)
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) mma_tf32(tmem, da + 2 * kk, db + 2 * kk, idesc, (it | kk) != 0);
+    mma_commit(su32(&done));
+  }
+  __syncwarp();
+  mbar_wait(su32(&done), 0, g);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256) : "memory");
+}
 
 __global__ void k_dmma884(double* out, int iters) {
   double a = threadIdx.x * 1e-3, b = 1.0 + threadIdx.x * 1e-4;
@@ -99,4 +148,40 @@ extern "C" __attribute__((visibility("default"))) int rgf_peak_fp64(int device, 
   cudaFree(buf);
   if (e == cudaSuccess) e = cudaGetLastError();
   return (int)e;
+}
+
+// Measured dense TF32 tensor-core rate (TFLOP/s) of tcgen05.mma kind::tf32 on
+// `device` (one CTA per SM, M = 128, N = 256, K = 8).  Returns 0 on success,
+// -2 if a wait timed out, else the CUDA error code.
+extern "C" __attribute__((visibility("default"))) int rgf_peak_tf32(int device, double* out) {
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return (int)e;
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const uint32_t smem = 128 * 1024 + 1024;  // the operands use 48 KB; more keeps one CTA per SM
+  if ((e = cudaFuncSetAttribute(k_tf32_peak, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) != cudaSuccess)
+    return (int)e;
+  int* err = nullptr;
+  if ((e = cudaMalloc(&err, sizeof(int))) != cudaSuccess) return (int)e;
+  cudaMemset(err, 0, sizeof(int));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const int iters = 20000;
+  k_tf32_peak<<<sms, 128, smem>>>(64, err);
+  cudaEventRecord(e0);
+  k_tf32_peak<<<sms, 128, smem>>>(iters, err);
+  cudaEventRecord(e1);
+  e = cudaEventSynchronize(e1);
+  int herr = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&herr, err, sizeof(int), cudaMemcpyDeviceToHost);
+  float ms = 0.f;
+  if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+  if (e == cudaSuccess && ms > 0.f) *out = 2.0 * 128 * 256 * 8 * 4.0 * iters * (double)sms / (ms * 1e-3) / 1e12;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(err);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return (int)e;
+  return herr ? -2 : 0;
 }
