@@ -390,13 +390,19 @@ __global__ void k_mx_delta(double2* S, int64_t ldS, const int* pairs, int npairs
 namespace gjs {
 constexpr int BN = 128;                 // real columns per tile
 constexpr uint32_t CH = 16384;          // one operand K-chunk: 128 rows x 32 fp32 (128-byte rows)
+// A = V (hi, lo); B = U (hi, lo), which first holds the U product's left
+// operand realify_right(W'(J, tile columns)) in the same geometry
 constexpr uint32_t OFF_AH = 0, OFF_AL = 2 * CH, OFF_BH = 4 * CH, OFF_BL = 6 * CH;  // 32 KB each
 constexpr uint32_t OFF_WP = 8 * CH;     // W' tile: 4 chunks [chunk][row][32 fp32], unswizzled
-constexpr uint32_t OFF_WJC = 12 * CH;   // W'(J, tile columns): 32 x 64 float2
-constexpr uint32_t OFF_T = 13 * CH;     // T: 32 x (32 + 1) float2
-constexpr uint32_t SMEM = OFF_T + NB * (NB + 1) * 8 + 1024;
+constexpr uint32_t TU_CH = 8192;        // one K-chunk of the T image: 64 rows x 128 bytes
+constexpr uint32_t TU_HALF = 2 * TU_CH; // hi image, then lo image
+constexpr uint32_t TU_BYTES = 2 * TU_HALF;
+constexpr uint32_t OFF_TU = 12 * CH;    // the realified T image (right operand of the U product)
+constexpr uint32_t SMEM = OFF_TU + TU_BYTES + 1024;
+constexpr uint32_t TMEM_COLS = 256;     // update accumulator: columns [0, 128); U product: [128, 192)
 constexpr int TP = BN + 4;              // pitch of the epilogue staging tile (over the operands)
 static_assert(128 * TP * 4 <= OFF_WP, "staging tile");
+static_assert(SMEM <= 227 * 1024, "shared memory of one CTA");
 }  // namespace gjs
 
 __device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, int* status, long long timeout) {
@@ -423,9 +429,20 @@ __device__ unsigned long long g_mx_stamps[16];
       g_mx_stamps[i] = t_;                                                              \
     }                                                                                   \
   } while (0)
+#define MX_SSTAMP(i)                                                                    \
+  do {                                                                                  \
+    if (threadIdx.x == 0) {                                                             \
+      unsigned long long t_;                                                            \
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_));                           \
+      g_mx_stamps[10 + (i)] = t_;                                                       \
+    }                                                                                   \
+  } while (0)
 #else
 #define MX_STAMP(i) \
   do {              \
+  } while (0)
+#define MX_SSTAMP(i) \
+  do {               \
   } while (0)
 #endif
 
@@ -568,9 +585,34 @@ __device__ __forceinline__ void inv32_block(const float2* Mb, float2* Ts, float2
 // J' = [j1, j1 + jn1) and, at the last step of a slice, the next slice's
 // stencil, permittivity and right-lead block (its first pivot block is then
 // A_{n+1}(J', J') - g_n(J', J') [- G0_R(J', J')])
+// The pivot-block inverse T as the right operand of the step's U product
+// (U = T W'(J, :), computed on the tensor core as conj(U)^T in realified
+// form): image rows 2t = T(t, :) and 2t + 1 = i T(t, :), K = (re, im) of
+// column m, K-major with the 128-byte swizzle, 2 K-chunks of 64 rows; the tf32
+// hi image, then the lo image.  Ts: T in shared memory, row pitch ldt.
+__device__ __forceinline__ void publish_tu(const float2* Ts, int ldt, uint8_t* img, int tid) {
+  const int r = tid >> 3, cq = tid & 7;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int m = cq + 8 * q, kf = 2 * m, kc = kf >> 5, gq = (kf & 31) >> 2, ofs = (kf & 3) * 4;
+    const float2 t = Ts[r * ldt + m];
+#pragma unroll
+    for (int rr = 0; rr < 2; rr++) {
+      const int n = 2 * r + rr;
+      const float x0 = rr ? -t.y : t.x, x1 = rr ? t.x : t.y;
+      const uint32_t off = kc * gjs::TU_CH + n * 128 + ((gq ^ (n & 7)) << 4) + ofs;
+      const float h0 = tf32_hi(x0), h1 = tf32_hi(x1);
+      *reinterpret_cast<float2*>(img + off) = make_float2(h0, h1);
+      *reinterpret_cast<float2*>(img + gjs::TU_HALF + off) = make_float2(x0 - h0, x1 - h1);
+    }
+  }
+}
+
 struct GjNext {
   const float2* Tin;
   float2* Tout;
+  const uint8_t* tu_in;  // image of Tin (publish_tu)
+  uint8_t* tu_out;       // image of Tout
   int j1, jn1;
   int next_slice;        // 1: J' is the next slice's first block
   int same_block;        // 1: J' is the current block (one block per slice)
@@ -643,6 +685,7 @@ __device__ void t_server(const float* __restrict__ Wsrc, int64_t lda, int j0, in
   inv32_block(Mn, To, tmp, jn1, tid, bad);
 #pragma unroll
   for (int q = 0; q < 4; q++) ns.Tout[r * NB + cq + 8 * q] = To[r * LD + cq + 8 * q];
+  publish_tu(To, LD, ns.tu_out, tid);
 }
 
 __global__ void __launch_bounds__(256, 1)
@@ -652,6 +695,8 @@ __global__ void __launch_bounds__(256, 1)
   using namespace gjs;
   extern __shared__ uint8_t smem_raw[];
   __shared__ __align__(8) uint64_t bar_ld;
+  __shared__ __align__(8) uint64_t bar_tu;
+  __shared__ __align__(8) uint64_t bar_mu;
   __shared__ __align__(8) uint64_t bar_mma;
   __shared__ uint32_t tmem_sh;
   __shared__ int bad;
@@ -664,15 +709,19 @@ __global__ void __launch_bounds__(256, 1)
     if (blockIdx.y != 0) return;
     if (tid == 0) bad = 0;
     pdl_wait();
+    MX_SSTAMP(0);
     __syncthreads();
     if (ns.Tout) t_server(Wsrc, lda, j0, jn, ns, gb, &bad);
     __syncthreads();
+    MX_SSTAMP(1);
     if (bad && tid == 0) atomicOr(status, kStatusSingular);
     return;
   }
   const int m0 = blockIdx.y * 128, n0 = blockIdx.x * BN;
   if (tid == 0) {
     tc32::mbar_init(tc32::su32(&bar_ld), 1);
+    tc32::mbar_init(tc32::su32(&bar_tu), 1);
+    tc32::mbar_init(tc32::su32(&bar_mu), 1);
     tc32::mbar_init(tc32::su32(&bar_mma), 1);
     bad = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -680,7 +729,7 @@ __global__ void __launch_bounds__(256, 1)
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc32::su32(&tmem_sh)),
-                 "r"(BN)
+                 "r"(TMEM_COLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -691,43 +740,82 @@ __global__ void __launch_bounds__(256, 1)
   pdl_wait();
   MX_STAMP(1);
 
-  // (1) TMA: V's rows W_src(m0.., 2 j0 .. 2 j0 + 63) swizzled for the MMA, and the W' tile
-  const uint32_t bl = tc32::su32(&bar_ld);
+  // (1) the image of this step's pivot-block inverse (published by the server
+  //     of the step before); TMA: V's rows W_src(m0.., 2 j0 .. 2 j0 + 63)
+  //     swizzled for the MMA, and the W' tile
+  const uint32_t bl = tc32::su32(&bar_ld), btu = tc32::su32(&bar_tu);
   if (tid == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(btu), "r"(TU_BYTES) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     sb + OFF_TU),
+                 "l"(ns.tu_in), "r"(TU_BYTES), "r"(btu)
+                 : "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bl), "r"(6 * CH) : "memory");
     for (int kc = 0; kc < 2; kc++) tc32::tma_load_3d(sb + OFF_AH + kc * CH, &mapA, 2 * j0 + 32 * kc, m0, 0, bl);
     for (int kc = 0; kc < 4; kc++) tc32::tma_load_3d(sb + OFF_WP + kc * CH, &mapW, n0 + 32 * kc, m0, 0, bl);
   }
-  // (2) this step's pivot-block inverse (from the server of the step before)
-  //     and W(J, tile columns) into registers
-  float2* Ts = reinterpret_cast<float2*>(gb + OFF_T);
+  // (2) the U product's left operand realify_right(W'(J, tile columns)), W' =
+  //     W with the pivot columns replaced by the identity's: lane = pivot row m
+  //     (K = 2m, 2m + 1), warp = 8 complex columns j (rows 2j: conj W'(m, j),
+  //     2j + 1: i conj W'(m, j)), split hi/lo into the B area
   {
-    const int r = tid >> 3, cq = tid & 7;
+    const int m = lane, kf = 2 * m, kc = kf >> 5, gq = (kf & 31) >> 2, ofs = (kf & 3) * 4;
+    float4 wv[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) Ts[r * (NB + 1) + cq + 8 * q] = ns.Tin[r * NB + cq + 8 * q];
-  }
-  float4 wj[4];
-#pragma unroll
-  for (int u = 0; u < 4; u++) {
-    const int e = tid + 256 * u, row = e >> 5, n = n0 + 4 * (e & 31);
-    wj[u] = (row < jn && n < lda) ? *reinterpret_cast<const float4*>(Wsrc + (int64_t)(j0 + row) * lda + n)
+    for (int q = 0; q < 4; q++) {
+      const int n = n0 + 16 * warp + 4 * q;
+      wv[q] = (m < jn && n < lda) ? *reinterpret_cast<const float4*>(Wsrc + (int64_t)(j0 + m) * lda + n)
                                   : make_float4(0.f, 0.f, 0.f, 0.f);
-  }
-  MX_STAMP(2);
-  MX_STAMP(3);
-  // W'(J, tile columns): the pivot columns replaced by the identity's
-  float2* Wj = reinterpret_cast<float2*>(gb + OFF_WJC);
+    }
+    MX_STAMP(2);
 #pragma unroll
-  for (int u = 0; u < 4; u++) {
-    const int e = tid + 256 * u, row = e >> 5, l = 2 * (e & 31);
-    const int c = (n0 >> 1) + l;
-    float2 v0 = make_float2(wj[u].x, wj[u].y), v1 = make_float2(wj[u].z, wj[u].w);
-    if (c >= j0 && c < j0 + jn) v0 = make_float2((j0 + row == c && row < jn) ? 1.f : 0.f, 0.f);
-    if (c + 1 >= j0 && c + 1 < j0 + jn) v1 = make_float2((j0 + row == c + 1 && row < jn) ? 1.f : 0.f, 0.f);
-    Wj[row * 64 + l] = v0;
-    Wj[row * 64 + l + 1] = v1;
+    for (int q = 0; q < 4; q++) {
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int j = 8 * warp + 2 * q + h, c = (n0 >> 1) + j;
+        float re = h ? wv[q].z : wv[q].x, im = h ? wv[q].w : wv[q].y;
+        if (c >= j0 && c < j0 + jn) {
+          re = (j0 + m == c && m < jn) ? 1.f : 0.f;
+          im = 0.f;
+        }
+#pragma unroll
+        for (int rr = 0; rr < 2; rr++) {
+          const int n = 2 * j + rr;
+          const float x0 = rr ? im : re, x1 = rr ? re : -im;
+          const uint32_t off = kc * CH + n * 128 + ((gq ^ (n & 7)) << 4) + ofs;
+          const float h0 = tf32_hi(x0), h1 = tf32_hi(x1);
+          *reinterpret_cast<float2*>(gb + OFF_BH + off) = make_float2(h0, h1);
+          *reinterpret_cast<float2*>(gb + OFF_BL + off) = make_float2(x0 - h0, x1 - h1);
+        }
+      }
+    }
   }
-  // (4) V = W(:, J) - E_J, split hi/lo in place over the swizzled TMA tile
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // operand writes -> tensor core
+  __syncthreads();
+  MX_STAMP(3);
+  // (3) the U product on tcgen05 (3xTF32, M = 128, N = 64, K = 64) into TMEM
+  //     columns [128, 192): row n of the result is row n of U's operand
+  const uint32_t bmu = tc32::su32(&bar_mu);
+  if (tid == 0) {
+    wait_bar(btu, 0, status, timeout);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+    for (int kc = 0; kc < 2; kc++) {
+      const uint64_t ah = tc32::sw128_desc(sb + OFF_BH + kc * CH), al = tc32::sw128_desc(sb + OFF_BL + kc * CH);
+      const uint64_t th = tc32::sw128_desc(sb + OFF_TU + kc * TU_CH);
+      const uint64_t tl = tc32::sw128_desc(sb + OFF_TU + TU_HALF + kc * TU_CH);
+#pragma unroll
+      for (int kk = 0; kk < 4; kk++) {
+        const uint64_t o = (uint64_t)(kk * 2);
+        tc32::mma_tf32(tmem + 128, al + o, th + o, tc32::Cfg<64>::IDESC, (kc | kk) != 0);
+        tc32::mma_tf32(tmem + 128, ah + o, tl + o, tc32::Cfg<64>::IDESC, 1);
+        tc32::mma_tf32(tmem + 128, ah + o, th + o, tc32::Cfg<64>::IDESC, 1);
+      }
+    }
+    tc32::mma_commit(bmu);
+  }
+  __syncwarp();
+  // (4) V = W(:, J) - E_J, split hi/lo in place over the swizzled TMA tile (while the U product runs)
   const bool ok_ld = wait_bar(bl, 0, status, timeout);
   MX_STAMP(4);
 #pragma unroll
@@ -743,43 +831,34 @@ __global__ void __launch_bounds__(256, 1)
     *reinterpret_cast<float4*>(gb + off) = h;
     *reinterpret_cast<float4*>(gb + off + (OFF_AL - OFF_AH)) = make_float4(x.x - h.x, x.y - h.y, x.z - h.z, x.w - h.w);
   }
-  __syncthreads();
   MX_STAMP(5);
-  // (5) U = T W'(J, tile columns): lane = row t of U, warp = 8 complex columns; written as
-  //     the MMA's right operand (rows 2l, 2l+1; K = 2t, 2t+1), 128-byte swizzle, hi/lo
+  // (5) the update's right operand from TMEM: row n (= tile column n) holds
+  //     (Re U(t, j), -Im U(t, j)) for n = 2j and (Im U, Re U) for n = 2j + 1
+  //     over K = 2t, 2t + 1; split hi/lo over the U product's left operand,
+  //     which the completed product no longer reads.  Warp w: rows
+  //     32 (w mod 4) .., K-chunk w / 4.
+  const bool ok_u = wait_bar(bmu, 0, status, timeout);
+  __syncwarp();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   {
-    float2 acc[8];
+    const int n = 32 * (warp & 3) + lane, kc = warp >> 2;
 #pragma unroll
-    for (int v = 0; v < 8; v++) acc[v] = make_float2(0.f, 0.f);
-    const float4* Wj4 = reinterpret_cast<const float4*>(Wj) + warp * 4;  // 8 complex = 4 float4 per row
-#pragma unroll 8
-    for (int sr = 0; sr < NB; sr++) {
-      const float2 tv = Ts[lane * (NB + 1) + sr];
+    for (int hf = 0; hf < 2; hf++) {
+      float v[16];
+      tc32::tmem_ld16(tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(128 + 32 * kc + 16 * hf), v);
 #pragma unroll
-      for (int v2 = 0; v2 < 4; v2++) {
-        const float4 w = Wj4[sr * 32 + v2];  // broadcast: every lane reads the same row of W'(J, :)
-        acc[2 * v2].x = fmaf(tv.x, w.x, fmaf(-tv.y, w.y, acc[2 * v2].x));
-        acc[2 * v2].y = fmaf(tv.x, w.y, fmaf(tv.y, w.x, acc[2 * v2].y));
-        acc[2 * v2 + 1].x = fmaf(tv.x, w.z, fmaf(-tv.y, w.w, acc[2 * v2 + 1].x));
-        acc[2 * v2 + 1].y = fmaf(tv.x, w.w, fmaf(tv.y, w.z, acc[2 * v2 + 1].y));
-      }
-    }
-    const int kf = 2 * lane, kc = kf >> 5, kk = kf & 31, gq = kk >> 2, ofs = (kk & 3) * 4;
-#pragma unroll
-    for (int v = 0; v < 8; v++) {
-      const int l = warp * 8 + v;
-#pragma unroll
-      for (int hh = 0; hh < 2; hh++) {
-        const int n = 2 * l + hh;
-        const float x0 = hh ? acc[v].y : acc[v].x, x1 = hh ? acc[v].x : -acc[v].y;
-        const uint32_t off = kc * CH + n * 128 + ((gq ^ (n & 7)) << 4) + ofs;
-        const float h0 = tf32_hi(x0), h1 = tf32_hi(x1);
-        *reinterpret_cast<float2*>(gb + OFF_BH + off) = make_float2(h0, h1);
-        *reinterpret_cast<float2*>(gb + OFF_BL + off) = make_float2(x0 - h0, x1 - h1);
+      for (int g4 = 0; g4 < 4; g4++) {
+        const int g = 4 * hf + g4;
+        const float4 x = make_float4(v[4 * g4], v[4 * g4 + 1], v[4 * g4 + 2], v[4 * g4 + 3]);
+        const float4 h = make_float4(tf32_hi(x.x), tf32_hi(x.y), tf32_hi(x.z), tf32_hi(x.w));
+        const uint32_t off = kc * CH + n * 128 + ((g ^ (n & 7)) << 4);
+        *reinterpret_cast<float4*>(gb + OFF_BH + off) = h;
+        *reinterpret_cast<float4*>(gb + OFF_BL + off) = make_float4(x.x - h.x, x.y - h.y, x.z - h.z, x.w - h.w);
       }
     }
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // operand writes -> tensor core
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   MX_STAMP(6);
   // (6) 2 K-chunks x 4 K-steps x 3 products on tcgen05
@@ -801,7 +880,7 @@ __global__ void __launch_bounds__(256, 1)
     tc32::mma_commit(bm);
   }
   __syncwarp();
-  const bool ok = wait_bar(bm, 0, status, timeout) && ok_ld;
+  const bool ok = wait_bar(bm, 0, status, timeout) && ok_ld && ok_u;
   MX_STAMP(7);
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   // (7) epilogue: D (TMEM) -> staging over the operands -> W_dst = W' - D, one warp per row
@@ -844,13 +923,13 @@ __global__ void __launch_bounds__(256, 1)
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
 }
 
 // the first pivot-block inverse of the first slice (later ones come from the
 // step kernels' server): T = W(J0, J0)^-1, one CTA
 __global__ void __launch_bounds__(256) k_mx_t0(const float* __restrict__ W, int64_t lda, int jn, float2* Tout,
-                                               int* status) {
+                                               uint8_t* tu_out, int* status) {
   pdl_open();
   pdl_wait();
   constexpr int LD = NB + 1;
@@ -870,6 +949,7 @@ __global__ void __launch_bounds__(256) k_mx_t0(const float* __restrict__ W, int6
   inv32_block(Mb, To, tmp, jn, tid, &bad);
 #pragma unroll
   for (int q = 0; q < 4; q++) Tout[r * NB + cq + 8 * q] = To[r * LD + cq + 8 * q];
+  publish_tu(To, LD, tu_out, tid);
   if (bad && tid == 0) atomicOr(status, kStatusSingular);
 }
 
@@ -916,6 +996,7 @@ size_t mixed_workspace_bytes(int64_t N, int64_t L, int64_t P) {
   b += sizeof(float2) * N * P * 148;          // partials (at most one per SM)
   b += 2 * sizeof(float) * 2 * P * lda;       // Bt hi/lo
   b += sizeof(double2) * N * P * 6;           // Bl, Br, b0, bL, e0/e1 (also G0 (B + x) at the end)
+  b += 4 * (sizeof(float2) * NB * NB + gjs::TU_BYTES);  // pivot-block inverses and their images
   return b;
 }
 
@@ -951,7 +1032,7 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
   int sTiles = (int)((2 * P + sbn - 1) / sbn);
   int sSplit = choose_ksplit((int64_t)ntile_m * sTiles, kchunks, sms / nside);
   if ((st = alloc(kMxW, 2 * nside * sizeof(float) * N * lda, &pW)) ||
-      (st = alloc(kMxT, sizeof(float2) * 2 * nside * NB * NB, &pT)) ||
+      (st = alloc(kMxT, (sizeof(float2) * NB * NB + gjs::TU_BYTES) * 2 * nside, &pT)) ||
       (st = alloc(kMxStoreHi, sizeof(float) * N * lda * L, &pSh)) ||
       (st = alloc(kMxStoreLo, sizeof(float) * N * lda * L, &pSl)) ||
       (st = alloc(kMxX, sizeof(double2) * NP * L, &pX)) || (st = alloc(kMxY, sizeof(float2) * NP * L, &pY)) ||
@@ -982,6 +1063,7 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
     float* W[2];
     CUtensorMap mA[2], mWp[2], mBh, mBl;
     float2* Tb;
+    uint8_t* Tu;  // images of the two inverses (publish_tu)
     float* bh;
     float* bl;
     float2* part;
@@ -998,6 +1080,7 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
     d.W[0] = static_cast<float*>(pW) + (2 * q) * N * lda;
     d.W[1] = d.W[0] + N * lda;
     d.Tb = static_cast<float2*>(pT) + 2 * q * NB * NB;
+    d.Tu = static_cast<uint8_t*>(pT) + sizeof(float2) * NB * NB * 2 * nside + 2 * q * gjs::TU_BYTES;
     d.bh = bt_hi + q * 4 * P * lda;
     d.bl = d.bh + 2 * P * lda;
     d.part = static_cast<float2*>(pPart) + q * NP * sSplit;
@@ -1089,7 +1172,7 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
   };
   auto first_t = [&](Side& d) {
     launch_pdl(k_mx_t0, dim3(1), dim3(256), 0, d.q, (const float*)d.W[d.cur], lda, (int)std::min<int64_t>(NB, N),
-               d.Tb + (d.gstep & 1) * NB * NB, mstat);
+               d.Tb + (d.gstep & 1) * NB * NB, d.Tu + (d.gstep & 1) * gjs::TU_BYTES, mstat);
     nl++;
   };
   // one Gauss-Jordan step of side d's slice k; knext: the slice whose first
@@ -1099,6 +1182,8 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
     GjNext ns{};
     ns.Tin = d.Tb + (d.gstep & 1) * NB * NB;
     ns.Tout = d.Tb + ((d.gstep + 1) & 1) * NB * NB;
+    ns.tu_in = d.Tu + (d.gstep & 1) * gjs::TU_BYTES;
+    ns.tu_out = d.Tu + ((d.gstep + 1) & 1) * gjs::TU_BYTES;
     ns.st_col = mp.st_col;
     ns.st_val = mp.st_val;
     ns.k2 = mp.k2;
