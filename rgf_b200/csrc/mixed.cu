@@ -429,12 +429,26 @@ __device__ unsigned long long g_mx_stamps[16];
       g_mx_stamps[i] = t_;                                                              \
     }                                                                                   \
   } while (0)
+// per launch (in launch order, up to 512): server phase times [0, 10), tile (0, 0) start/end [14, 16)
+__device__ unsigned long long g_mx_tl[512][16];
+__device__ unsigned int g_mx_tl_n[2];
 #define MX_SSTAMP(i)                                                                    \
   do {                                                                                  \
     if (threadIdx.x == 0) {                                                             \
       unsigned long long t_;                                                            \
       asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_));                           \
       g_mx_stamps[10 + (i)] = t_;                                                       \
+      if ((i) == 0) mx_sslot = atomicAdd(&g_mx_tl_n[0], 1u) & 511u;                     \
+      g_mx_tl[mx_sslot][(i)] = t_;                                                      \
+    }                                                                                   \
+  } while (0)
+#define MX_TSTAMP(i)                                                                    \
+  do {                                                                                  \
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {                       \
+      unsigned long long t_;                                                            \
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_));                           \
+      if ((i) == 0) mx_tslot = atomicAdd(&g_mx_tl_n[1], 1u) & 511u;                     \
+      g_mx_tl[mx_tslot][14 + (i)] = t_;                                                 \
     }                                                                                   \
   } while (0)
 #else
@@ -443,6 +457,16 @@ __device__ unsigned long long g_mx_stamps[16];
   } while (0)
 #define MX_SSTAMP(i) \
   do {               \
+  } while (0)
+#define MX_TSTAMP(i) \
+  do {               \
+  } while (0)
+#endif
+#ifdef RGF_MX_STAMPS
+#define MX_DECL unsigned mx_sslot = 0, mx_tslot = 0
+#else
+#define MX_DECL \
+  do {          \
   } while (0)
 #endif
 
@@ -512,33 +536,42 @@ __device__ __forceinline__ void mm16(const float2* A, int lda_, const float2* B,
 }
 
 // C (32 x 32) = sign * A B (+ D) in shared memory (leading dimension 33) by
-// 256 threads: thread t computes row t/8, columns t%8 + 8q
+// 256 threads: thread t computes rows i, i + 16 and columns c, c + 16
+// (i = t / 16, c = t % 16)
 __device__ __forceinline__ void mm32(const float2* A, const float2* B, const float2* D, float sign, float2* C,
                                      int t) {
   constexpr int LD = NB + 1;
-  const int i = t >> 3, c0 = t & 7;
-  float2 acc[4];
+  const int i = t >> 4, c = t & 15;
+  float2 acc[2][2];
 #pragma unroll
-  for (int q = 0; q < 4; q++) acc[q] = make_float2(0.f, 0.f);
+  for (int u = 0; u < 2; u++)
+#pragma unroll
+    for (int v = 0; v < 2; v++) acc[u][v] = make_float2(0.f, 0.f);
 #pragma unroll 8
   for (int s = 0; s < NB; s++) {
-    const float2 av = A[i * LD + s];
+    const float2 a0 = A[i * LD + s], a1 = A[(i + 16) * LD + s];
+    const float2 b0 = B[s * LD + c], b1 = B[s * LD + c + 16];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const float2 u = fcmul(av, B[s * LD + c0 + 8 * q]);
-      acc[q].x += u.x;
-      acc[q].y += u.y;
-    }
+    for (int u = 0; u < 2; u++)
+#pragma unroll
+      for (int v = 0; v < 2; v++) {
+        const float2 av = u ? a1 : a0, bv = v ? b1 : b0;
+        acc[u][v].x = fmaf(av.x, bv.x, fmaf(-av.y, bv.y, acc[u][v].x));
+        acc[u][v].y = fmaf(av.x, bv.y, fmaf(av.y, bv.x, acc[u][v].y));
+      }
   }
 #pragma unroll
-  for (int q = 0; q < 4; q++) {
-    float2 v = make_float2(sign * acc[q].x, sign * acc[q].y);
-    if (D) {
-      v.x += D[i * LD + c0 + 8 * q].x;
-      v.y += D[i * LD + c0 + 8 * q].y;
+  for (int u = 0; u < 2; u++)
+#pragma unroll
+    for (int v = 0; v < 2; v++) {
+      const int o = (i + 16 * u) * LD + c + 16 * v;
+      float2 w = make_float2(sign * acc[u][v].x, sign * acc[u][v].y);
+      if (D) {
+        w.x += D[o].x;
+        w.y += D[o].y;
+      }
+      C[o] = w;
     }
-    C[i * LD + c0 + 8 * q] = v;
-  }
 }
 
 // T = M^-1 for the identity-padded 32 x 32 pivot block M (shared memory,
@@ -629,6 +662,20 @@ struct GjNext {
 // disjoint), or T itself when J' = J, assembled with the next slice's matrix
 // at a slice boundary, then its inverse into ns.Tout -- computed while the
 // tile CTAs apply this step, so that the next step starts with its T ready.
+#ifdef RGF_MX_STAMPS
+#define MX_PSTAMP(i)                                                                    \
+  do {                                                                                  \
+    if (threadIdx.x == 0) {                                                             \
+      unsigned long long t_;                                                            \
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_));                           \
+      g_mx_tl[(g_mx_tl_n[0] - 1u) & 511u][(i)] = t_;                                    \
+    }                                                                                   \
+  } while (0)
+#else
+#define MX_PSTAMP(i) \
+  do {               \
+  } while (0)
+#endif
 __device__ void t_server(const float* __restrict__ Wsrc, int64_t lda, int j0, int jn, const GjNext& ns,
                          uint8_t* gb, int* bad) {
   constexpr int LD = NB + 1;
@@ -652,9 +699,11 @@ __device__ void t_server(const float* __restrict__ Wsrc, int64_t lda, int j0, in
     B3[r * LD + c] = (r < jn1 && c < jn1) ? *reinterpret_cast<const float2*>(Wsrc + (int64_t)(j1 + r) * lda + 2 * (j1 + c)) : z;
   }
   __syncthreads();
+  MX_PSTAMP(2);
   if (!ns.same_block) {
     mm32(Tj, B1, nullptr, 1.f, U1, tid);  // U1 = T W(J, J')
     __syncthreads();
+    MX_PSTAMP(3);
     mm32(B2, U1, B3, -1.f, Mn, tid);      // W(J', J') - W(J', J) U1
   } else {
 #pragma unroll
@@ -682,7 +731,9 @@ __device__ void t_server(const float* __restrict__ Wsrc, int64_t lda, int j0, in
     Mn[r * LD + c] = v;
   }
   __syncthreads();
+  MX_PSTAMP(4);
   inv32_block(Mn, To, tmp, jn1, tid, bad);
+  MX_PSTAMP(5);
 #pragma unroll
   for (int q = 0; q < 4; q++) ns.Tout[r * NB + cq + 8 * q] = To[r * LD + cq + 8 * q];
   publish_tu(To, LD, ns.tu_out, tid);
@@ -701,6 +752,7 @@ __global__ void __launch_bounds__(256, 1)
   __shared__ uint32_t tmem_sh;
   __shared__ int bad;
   pdl_open();
+  MX_DECL;
   MX_STAMP(0);
   const uint32_t sb = (tc32::su32(smem_raw) + 1023u) & ~1023u;
   uint8_t* gb = smem_raw + (sb - tc32::su32(smem_raw));
@@ -739,6 +791,7 @@ __global__ void __launch_bounds__(256, 1)
   const uint32_t tmem = tmem_sh;
   pdl_wait();
   MX_STAMP(1);
+  MX_TSTAMP(0);
 
   // (1) the image of this step's pivot-block inverse (published by the server
   //     of the step before); TMA: V's rows W_src(m0.., 2 j0 .. 2 j0 + 63)
@@ -920,6 +973,7 @@ __global__ void __launch_bounds__(256, 1)
     }
   }
   MX_STAMP(9);
+  MX_TSTAMP(1);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
@@ -983,6 +1037,12 @@ int choose_ksplit(int64_t tiles, int64_t kchunks, int sms) {
 #ifdef RGF_MX_STAMPS
 extern "C" __attribute__((visibility("default"))) int rgf_dev_mx_stamps(unsigned long long* out) {
   return (int)cudaMemcpyFromSymbol(out, g_mx_stamps, sizeof(g_mx_stamps));
+}
+extern "C" __attribute__((visibility("default"))) int rgf_dev_mx_timeline(unsigned long long* out, unsigned* n) {
+  cudaMemcpyFromSymbol(n, g_mx_tl_n, sizeof(g_mx_tl_n));
+  const unsigned z[2] = {0, 0};
+  cudaMemcpyToSymbol(g_mx_tl_n, z, sizeof(z));
+  return (int)cudaMemcpyFromSymbol(out, g_mx_tl, sizeof(g_mx_tl));
 }
 #endif
 
