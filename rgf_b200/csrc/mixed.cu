@@ -1068,11 +1068,6 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  // solve GEMM tile width: 64 real columns for narrow requests, else 128 (a
-  // three-deep TMA pipeline; 256-wide tiles leave room for two stages only
-  // and stall on the loads)
-  const int sbn = (2 * P <= 64) ? 64 : 128;
-  if ((st = gemm_attr<64>()) || (st = gemm_attr<128>()) || (st = gemm_attr<256>())) return st;
   if (cudaFuncSetAttribute(k_mx_gj_step, cudaFuncAttributeMaxDynamicSharedMemorySize, gjs::SMEM) != cudaSuccess) {
     set_error("cannot configure the Gauss-Jordan step kernel's shared memory");
     return RGF_ERR_CUDA;
@@ -1089,6 +1084,12 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
   const bool two = L >= 8;
   const int64_t cj = two ? (L + 1) / 2 : L;  // junction slice + 1 (two-sided)
   const int nside = two ? 2 : 1;
+  // solve GEMM tile width: 64 real columns for narrow requests, else 128 (a
+  // three-deep TMA pipeline).  Measured slower at config 2 (2P = 408): 256-wide
+  // tiles (two stages only, stalled on the loads) and 3 tiles of 144 with a
+  // ragged 3-way K-split (780 ms of solves against 715 ms for 4 x 128, 2-way).
+  const int sbn = (2 * P <= 64) ? 64 : 128;
+  if ((st = gemm_attr<64>()) || (st = gemm_attr<128>())) return st;
   int sTiles = (int)((2 * P + sbn - 1) / sbn);
   int sSplit = choose_ksplit((int64_t)ntile_m * sTiles, kchunks, sms / nside);
   if ((st = alloc(kMxW, 2 * nside * sizeof(float) * N * lda, &pW)) ||

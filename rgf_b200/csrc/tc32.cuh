@@ -51,6 +51,8 @@ enum : int { kErrTimeout = 4 };
 struct GemmArgs {
   int M, Nr;               // rows of D, real columns of D
   int k_chunks;            // BK-chunks of K per CTA (one K-split)
+  int k_total;             // > 0: ragged K-split instead, split z of Z taking the chunks
+                           // [z k_total / Z, (z + 1) k_total / Z) (k_chunks unused)
   int a_z, b_z;            // batch coordinate (3rd tensor-map dimension) of A and B
   int mode;
   float* out;              // row-major fp32
@@ -62,15 +64,18 @@ struct GemmArgs {
   const int* az_dev;       // non-null: a_z is added to *az_dev (read after the grid before has finished)
 };
 
+// tile width BN: any multiple of 16 in [64, 256] (the M = 128 MMA shape);
+// every stage buffer starts on a 1024-byte boundary (the swizzle atom)
 template <int BN>
 struct Cfg {
-  static_assert(BN == 64 || BN == 128 || BN == 256, "BN");
+  static_assert(BN % 16 == 0 && BN >= 64 && BN <= 256, "BN");
   static constexpr uint32_t A_BYTES = BM * BK * 4;
   static constexpr uint32_t B_BYTES = BN * BK * 4;
   static constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
-  static constexpr int STAGES = (int)((192u * 1024u) / STAGE_BYTES);
+  static constexpr int STAGES = (int)((224u * 1024u) / STAGE_BYTES);
+  static_assert(STAGES >= 2 && B_BYTES % 1024 == 0, "stages");
   static constexpr uint32_t SMEM = STAGES * STAGE_BYTES + 1024;  // + alignment slack
-  static constexpr uint32_t TMEM_COLS = BN < 32 ? 32 : BN;
+  static constexpr uint32_t TMEM_COLS = BN <= 64 ? 64 : (BN <= 128 ? 128 : 256);  // a power of two
   // instruction descriptor: D f32 (bits 4-5 = 1), A/B tf32 (bits 7-9, 10-12 = 2),
   // both K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28
   static constexpr uint32_t IDESC =
@@ -172,7 +177,11 @@ __global__ void __launch_bounds__(kThreads, 1)
   const uint32_t base = (su32(smem_raw) + 1023u) & ~1023u;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
-  const int kc0 = blockIdx.z * g.k_chunks;
+  int kc0 = blockIdx.z * g.k_chunks, nk = g.k_chunks;
+  if (g.k_total > 0) {
+    kc0 = (int)((int64_t)blockIdx.z * g.k_total / gridDim.z);
+    nk = (int)((int64_t)(blockIdx.z + 1) * g.k_total / gridDim.z) - kc0;
+  }
   int a_z = g.a_z;
   auto sA_hi = [&](int s) { return base + (uint32_t)s * C::STAGE_BYTES; };
   auto sA_lo = [&](int s) { return sA_hi(s) + C::A_BYTES; };
@@ -204,7 +213,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (warp == 0 && lane == 0) {
     // producer: one stage = A_hi, A_lo (BM rows) and B_hi, B_lo (BN rows) of BK floats
-    for (int kt = 0; kt < g.k_chunks; kt++) {
+    for (int kt = 0; kt < nk; kt++) {
       const int s = kt % S;
       if (kt >= S && !mbar_wait(su32(&empty_bar[s]), ((kt / S) - 1) & 1, g)) {
         abort_sh = 1;
@@ -221,7 +230,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issuer: 4 K-steps of 8 per stage, 3 products each
-    for (int kt = 0; kt < g.k_chunks; kt++) {
+    for (int kt = 0; kt < nk; kt++) {
       const int s = kt % S;
       if (!mbar_wait(su32(&full_bar[s]), (kt / S) & 1, g)) {
         abort_sh = 1;
@@ -252,7 +261,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   constexpr int TP = BN + 4;  // tile pitch in floats (row shift of 4 banks: conflict-free float4 stores)
   static_assert(BM * TP * 4 <= S * C::STAGE_BYTES, "epilogue tile");
   float* tile = reinterpret_cast<float*>(smem_raw + (base - su32(smem_raw)));
-  const bool run = ok && g.k_chunks > 0;
+  const bool run = ok && nk > 0;
   if (run) {
     const int row = warp * 32 + lane;
 #pragma unroll 1

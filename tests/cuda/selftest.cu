@@ -73,6 +73,7 @@ static int tc32_run(int M, int Nr, int K, int ksplit, int mode, int gj_c0, int g
     g.M = M;
     g.Nr = Nr;
     g.k_chunks = K / BK / ksplit;
+    if ((K / BK) % ksplit) g.k_total = K / BK;  // ragged K-split
     g.mode = mode;
     g.out = dout;
     g.ldo = Nr;
@@ -105,10 +106,12 @@ extern "C" __attribute__((visibility("default"))) int rgf_selftest_tc32(int M, i
                                                                         const float* a_hi, const float* a_lo,
                                                                         const float* b_hi, const float* b_lo,
                                                                         float* out) {
-  if (M < 1 || Nr < 1 || K < 32 || K % 32 || ksplit < 1 || (K / 32) % ksplit) return -3;
+  if (M < 1 || Nr < 1 || K < 32 || K % 32 || ksplit < 1 || ksplit > K / 32) return -3;
   switch (bn) {
     case 64: return tc32_run<64>(M, Nr, K, ksplit, mode, gj_c0, gj_nb, a_hi, a_lo, b_hi, b_lo, out);
     case 128: return tc32_run<128>(M, Nr, K, ksplit, mode, gj_c0, gj_nb, a_hi, a_lo, b_hi, b_lo, out);
+    case 144: return tc32_run<144>(M, Nr, K, ksplit, mode, gj_c0, gj_nb, a_hi, a_lo, b_hi, b_lo, out);
+    case 208: return tc32_run<208>(M, Nr, K, ksplit, mode, gj_c0, gj_nb, a_hi, a_lo, b_hi, b_lo, out);
     case 256: return tc32_run<256>(M, Nr, K, ksplit, mode, gj_c0, gj_nb, a_hi, a_lo, b_hi, b_lo, out);
   }
   return -3;

@@ -68,7 +68,8 @@ def rel(a, b):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("M,Kc,Nc,bn", [(128, 16, 32, 64), (256, 64, 96, 64), (200, 48, 68, 128),
-                                         (384, 32, 128, 256), (130, 80, 200, 128)])
+                                         (384, 32, 128, 256), (130, 80, 200, 128), (256, 64, 204, 144),
+                                         (130, 48, 100, 208)])
 def test_complex_product(M, Kc, Nc, bn):
     rng = np.random.default_rng(M + Kc + Nc)
     P = (rng.standard_normal((M, Kc)) + 1j * rng.standard_normal((M, Kc))).astype(np.complex64)
@@ -95,6 +96,23 @@ def test_ksplit_partials():
     assert rel(out.sum(axis=0, dtype=np.float64), ref) < 3e-6
     for z in range(4):  # each split is its own quarter of K
         refz = A[:, z * 128:(z + 1) * 128].astype(np.float64) @ Bt[:, z * 128:(z + 1) * 128].astype(np.float64).T
+        assert rel(out[z], refz) < 3e-6
+
+
+@pytest.mark.gpu
+def test_ragged_ksplit_partials():
+    """A K-split that does not divide the chunk count (16 chunks in 3 splits:
+    5, 5, 6 chunks of 32) on 144-wide tiles, as the refinement's solve uses."""
+    rng = np.random.default_rng(8)
+    M, K, Nr = 256, 512, 408
+    A = rng.standard_normal((M, K)).astype(np.float32)
+    Bt = rng.standard_normal((Nr, K)).astype(np.float32)
+    out = run(A, Bt, 144, ksplit=3, mode=K_PARTIAL)
+    ref = A.astype(np.float64) @ Bt.astype(np.float64).T
+    assert rel(out.sum(axis=0, dtype=np.float64), ref) < 3e-6
+    for z in range(3):
+        lo, hi = 32 * (z * 16 // 3), 32 * ((z + 1) * 16 // 3)
+        refz = A[:, lo:hi].astype(np.float64) @ Bt[:, lo:hi].astype(np.float64).T
         assert rel(out[z], refz) < 3e-6
 
 
