@@ -423,7 +423,7 @@ __device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, int* sta
 __device__ unsigned long long g_mx_stamps[16];
 #define MX_STAMP(i)                                                                     \
   do {                                                                                  \
-    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {                       \
+    if (blockIdx.x == 1 && blockIdx.y == 0 && threadIdx.x == 0) {                       \
       unsigned long long t_;                                                            \
       asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_));                           \
       g_mx_stamps[i] = t_;                                                              \
@@ -444,7 +444,7 @@ __device__ unsigned int g_mx_tl_n[2];
   } while (0)
 #define MX_TSTAMP(i)                                                                    \
   do {                                                                                  \
-    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {                       \
+    if (blockIdx.x == 1 && blockIdx.y == 0 && threadIdx.x == 0) {                       \
       unsigned long long t_;                                                            \
       asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_));                           \
       if ((i) == 0) mx_tslot = atomicAdd(&g_mx_tl_n[1], 1u) & 511u;                     \
@@ -757,7 +757,10 @@ __global__ void __launch_bounds__(256, 1)
   const uint32_t sb = (tc32::su32(smem_raw) + 1023u) & ~1023u;
   uint8_t* gb = smem_raw + (sb - tc32::su32(smem_raw));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  if (blockIdx.x == gridDim.x - 1) {  // the last grid column: the pivot-block server (row 0) only
+  // grid column 0: the pivot-block server (row 0) only -- the first CTA of the
+  // grid to be scheduled, so that it never waits for an SM behind tiles (of
+  // this grid or of the other side's)
+  if (blockIdx.x == 0) {
     if (blockIdx.y != 0) return;
     if (tid == 0) bad = 0;
     pdl_wait();
@@ -769,7 +772,7 @@ __global__ void __launch_bounds__(256, 1)
     if (bad && tid == 0) atomicOr(status, kStatusSingular);
     return;
   }
-  const int m0 = blockIdx.y * 128, n0 = blockIdx.x * BN;
+  const int m0 = blockIdx.y * 128, n0 = (blockIdx.x - 1) * BN;
   if (tid == 0) {
     tc32::mbar_init(tc32::su32(&bar_ld), 1);
     tc32::mbar_init(tc32::su32(&bar_tu), 1);
@@ -1209,7 +1212,7 @@ rgf_status smatrix_mixed(const MixedProblem& mp, const MixedAlloc& alloc, cudaSt
   // (1) low-precision factorization
   RGF_CUDA_TRY_MX(cudaEventRecord(ev[0], s));
   const dim3 ga((unsigned)((ldw + 255) / 256), (unsigned)std::min<int64_t>(N, 8192));
-  // one grid column more than the tiles: its first CTA serves the next pivot block
+  // one grid column more than the tiles (column 0): its first CTA serves the next pivot block
   const dim3 ggj((unsigned)((lda + gjs::BN - 1) / gjs::BN + 1), (unsigned)ntile_m);
   auto lead = [&](int64_t k, int side) -> const double2* {  // lead block in slice k's matrix
     if (side == 0) return (k == 0) ? mp.G0[0] : nullptr;
